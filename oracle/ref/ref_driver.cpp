@@ -1,0 +1,187 @@
+// ref_driver.cpp -- C entry points over the reference's own hot-path code, compiled in
+// place against the AMReX-API shim (test infrastructure: the oracle/_ref build).
+//
+// What runs is the reference: pc_umeth_3D (Source/Godunov.cpp:59-476, with trace_ppm
+// from Source/PPM.cpp) and the device-inline kernels of Source/Godunov.H, Hydro.H and
+// PeleCUtilities.H. Only the host-side orchestration of pc_umdrv / pc_adjust_fluxes /
+// pc_consup (Source/Hydro.cpp:304-413, 545-557) and the box loop body of
+// construct_hydro_source (Hydro.cpp:70-249) are restated here, because Hydro.cpp also
+// defines PeleC member functions that need the full AMReX/PeleC runtime. The timestep
+// reduction (Source/Timestep.H:51-88) is restated for the same reason (its header pulls
+// in the transport library).
+#include "Hydro.H"
+
+#include <cfloat>
+
+#include "pcg_oracle.h"
+
+namespace {
+
+amrex::Array4<amrex::Real> view(const orc_array4* a) {
+  return amrex::Array4<amrex::Real>(a->p, a->jstride, a->kstride, a->nstride,
+                                    amrex::Dim3{a->begin[0], a->begin[1], a->begin[2]},
+                                    amrex::Dim3{a->end[0], a->end[1], a->end[2]}, a->ncomp);
+}
+
+amrex::Box mkbox(const int32_t lo[3], const int32_t hi[3]) {
+  return amrex::Box(amrex::IntVect(lo[0], lo[1], lo[2]), amrex::IntVect(hi[0], hi[1], hi[2]));
+}
+
+// Source/Hydro.cpp:304-377 (pc_umdrv) with :380-413 (pc_adjust_fluxes) and :545-557
+// (pc_consup) inlined; every pointwise call is the reference's own function.
+int umdrv(const orc_params* prm, const amrex::Box& bx, amrex::Array4<const amrex::Real> uin,
+          amrex::Array4<amrex::Real> uout, amrex::Array4<const amrex::Real> q,
+          amrex::Array4<const amrex::Real> qaux, amrex::Array4<const amrex::Real> src_q,
+          const amrex::GpuArray<const amrex::Array4<amrex::Real>, 3>& flx,
+          const amrex::GpuArray<const amrex::Array4<const amrex::Real>, 3>& a,
+          amrex::Array4<amrex::Real> vol) {
+  if (prm->ppm_type != 0 && prm->ppm_type != 1) return -2;
+  const amrex::GpuArray<amrex::Real, 3> dx{{prm->dx[0], prm->dx[1], prm->dx[2]}};
+  auto const& bxg2 = grow(bx, 2);
+  amrex::FArrayBox qec[3];
+  for (int dir = 0; dir < 3; dir++) qec[dir].resize(amrex::surroundingNodes(bxg2, dir), NGDNV);
+  amrex::GpuArray<const amrex::Array4<amrex::Real>, 3> qec_arr{{qec[0].array(), qec[1].array(), qec[2].array()}};
+  amrex::FArrayBox divu(bxg2, 1);
+  amrex::FArrayBox pdivu(bx, 1);
+  auto const& divuarr = divu.array();
+  auto const& pdivuarr = pdivu.array();
+
+  pc_umeth_3D(bx, prm->bclo, prm->bchi, prm->domlo, prm->domhi, q, qaux, src_q, flx, qec_arr, a, pdivuarr,
+              vol, dx, prm->dt, prm->ppm_type, prm->plm_iorder, prm->use_flattening != 0,
+              prm->use_hybrid_weno != 0, prm->weno_scheme);
+
+  amrex::ParallelFor(bxg2, [=](int i, int j, int k) { pc_divu(i, j, k, q, dx[0], dx[1], dx[2], divuarr); });
+
+  for (int dir = 0; dir < 3; dir++) {
+    amrex::Box const& fbx = amrex::surroundingNodes(bx, dir);
+    const amrex::Real dxd = dx[dir];
+    const int domlo_dir = prm->domlo[dir];
+    const int domhi_dir = prm->domhi[dir];
+    const int bclo_dir = prm->bclo[dir];
+    const int bchi_dir = prm->bchi[dir];
+    const amrex::Real difmag = prm->difmag;
+    amrex::ParallelFor(fbx, [=](int i, int j, int k) {
+      pc_artif_visc(i, j, k, flx[dir], divuarr, uin, dxd, difmag, dir, domlo_dir, domhi_dir, bclo_dir, bchi_dir);
+      pc_norm_spec_flx(i, j, k, flx[dir]);
+      pc_ext_flx(i, j, k, flx[dir], a[dir]);
+    });
+  }
+  amrex::ParallelFor(bx, [=](int i, int j, int k) { pc_update(i, j, k, uout, flx, vol, pdivuarr); });
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int ref_nspec(void) { return NUM_SPECIES; }
+
+int ref_set_eos_gamma(double gamma, double mw) {
+  if (NUM_SPECIES != 1) return -1;
+  return orc_set_eos_gamma(gamma, mw);
+}
+
+int ref_set_eos_nasa7(int nspec, const double* mw, const double* tmid, const double* a_lo, const double* a_hi) {
+  if (nspec != NUM_SPECIES) return -1;
+  return orc_set_eos_nasa7(nspec, mw, tmid, a_lo, a_hi);
+}
+
+int ref_ctoprim(const int32_t lo[3], const int32_t hi[3], const orc_array4* u, orc_array4* q, orc_array4* qaux) {
+  auto ua = view(u);
+  auto qa = view(q);
+  auto aa = view(qaux);
+  amrex::Array4<const amrex::Real> uc = ua;
+  amrex::ParallelFor(mkbox(lo, hi), [=](int i, int j, int k) { pc_ctoprim(i, j, k, uc, qa, aa); });
+  return 0;
+}
+
+int ref_umdrv(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], const orc_array4* uin,
+              orc_array4* uout, const orc_array4* q, const orc_array4* qaux, const orc_array4* srcq,
+              orc_array4* flx, const orc_array4* area, const orc_array4* vol) {
+  if (prm->nspec != NUM_SPECIES) return -3;
+  const amrex::Box bx = mkbox(lo, hi);
+  amrex::FArrayBox zero_src;
+  amrex::Array4<const amrex::Real> sq;
+  if (srcq) {
+    sq = view(srcq);
+  } else {
+    zero_src.resize(grow(bx, 4), QVAR);
+    sq = zero_src.const_array();
+  }
+  const amrex::GpuArray<const amrex::Array4<amrex::Real>, 3> f{{view(&flx[0]), view(&flx[1]), view(&flx[2])}};
+  const amrex::GpuArray<const amrex::Array4<const amrex::Real>, 3> a{{view(&area[0]), view(&area[1]), view(&area[2])}};
+  return umdrv(prm, bx, view(uin), view(uout), view(q), view(qaux), sq, f, a, view(vol));
+}
+
+// Source/Hydro.cpp:70-249 for one regular box, no sources (sources_for_hydro == 0).
+int ref_hydro_box(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], const orc_array4* uin,
+                  orc_array4* uout, orc_array4* flx, const orc_array4* area, const orc_array4* vol) {
+  if (prm->nspec != NUM_SPECIES) return -3;
+  const amrex::Box bx = mkbox(lo, hi);
+  const amrex::Box qbx = grow(bx, 4);
+  amrex::FArrayBox q(qbx, QVAR), qaux(qbx, NQAUX), src_q(qbx, QVAR), src_in(qbx, NVAR);
+  auto const& qarr = q.array();
+  auto const& qauxar = qaux.array();
+  auto const& srcqarr = src_q.array();
+  amrex::Array4<const amrex::Real> sarr = view(uin);
+  amrex::Array4<const amrex::Real> srcin = src_in.const_array();
+  amrex::ParallelFor(qbx, [=](int i, int j, int k) { pc_ctoprim(i, j, k, sarr, qarr, qauxar); });
+  amrex::ParallelFor(qbx, [=](int i, int j, int k) { pc_srctoprim(i, j, k, qarr, qauxar, srcin, srcqarr); });
+  auto hyd_src = view(uout);
+  amrex::ParallelFor(bx, [=](int i, int j, int k) {
+    for (int n = 0; n < NVAR; ++n) hyd_src(i, j, k, n) = 0.0;
+  });
+  amrex::GpuArray<const amrex::Array4<amrex::Real>, 3> f{{view(&flx[0]), view(&flx[1]), view(&flx[2])}};
+  for (int dir = 0; dir < 3; ++dir) {
+    auto fd = f[dir];
+    amrex::ParallelFor(amrex::surroundingNodes(bx, dir), [=](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) fd(i, j, k, n) = 0.0;
+    });
+  }
+  const amrex::GpuArray<const amrex::Array4<const amrex::Real>, 3> a{{view(&area[0]), view(&area[1]), view(&area[2])}};
+  return umdrv(prm, bx, sarr, hyd_src, q.const_array(), qaux.const_array(), src_q.const_array(), f, a, view(vol));
+}
+
+// Source/Timestep.H:51-88 (pc_estdt_hydro), regular cells.
+double ref_estdt(const int32_t lo[3], const int32_t hi[3], const orc_array4* u, const double dx[3]) {
+  auto ua = view(u);
+  double dt = std::numeric_limits<double>::max();
+  auto eos = pele::physics::PhysicsType::eos();
+  amrex::Loop(mkbox(lo, hi), [&](int i, int j, int k) {
+    const amrex::Real rho = ua(i, j, k, URHO);
+    const amrex::Real rhoInv = 1.0 / rho;
+    amrex::Real T = ua(i, j, k, UTEMP);
+    amrex::Real massfrac[NUM_SPECIES];
+    amrex::Real c;
+    for (int n = 0; n < NUM_SPECIES; ++n) massfrac[n] = ua(i, j, k, UFS + n) * rhoInv;
+    eos.RTY2Cs(rho, T, massfrac, c);
+    const amrex::Real ux = ua(i, j, k, UMX) * rhoInv;
+    dt = amrex::min<amrex::Real>(dt, dx[0] / (c + std::abs(ux)));
+    const amrex::Real uy = ua(i, j, k, UMY) * rhoInv;
+    dt = amrex::min<amrex::Real>(dt, dx[1] / (c + std::abs(uy)));
+    const amrex::Real uz = ua(i, j, k, UMZ) * rhoInv;
+    dt = amrex::min<amrex::Real>(dt, dx[2] / (c + std::abs(uz)));
+  });
+  return dt;
+}
+
+// Source/Advance.cpp:397-417 (construct_Snew, hydro only) then Source/PeleC.cpp:2289-2305
+// (computeTemp) with the reference's pc_rst_int_e and pc_cmpTemp.
+int ref_update_state(const int32_t lo[3], const int32_t hi[3], const orc_array4* s_old,
+                     const orc_array4* hydro_source, double dt, orc_array4* s_new) {
+  auto so = view(s_old);
+  auto hs = view(hydro_source);
+  auto sn = view(s_new);
+  const amrex::Box b = mkbox(lo, hi);
+  amrex::ParallelFor(b, [=](int i, int j, int k) {
+    for (int n = 0; n < NVAR; ++n) {
+      sn(i, j, k, n) = so(i, j, k, n);
+      sn(i, j, k, n) += dt * hs(i, j, k, n);
+    }
+  });
+  amrex::ParallelFor(b, [=](int i, int j, int k) { pc_rst_int_e(i, j, k, sn, true, true, false, 0.0); });
+  amrex::ParallelFor(b, [=](int i, int j, int k) { pc_cmpTemp(i, j, k, sn); });
+  return 0;
+}
+
+} // extern "C"

@@ -1,0 +1,190 @@
+/*
+ * pcg_hydro.h -- C ABI of the B200 (sm_100a) Godunov hydro advance.
+ *
+ * Drop-in for PeleC's unsplit Godunov path:
+ *   PeleC::construct_hydro_source  (Source/Hydro.cpp:4-301, Source/PeleC.H:340)
+ *     -> pc_ctoprim                (Source/Hydro.cpp:104-116, Source/PeleCUtilities.H:242-320)
+ *     -> pc_umdrv                  (Source/Hydro.cpp:304-377, declared Source/Hydro.H:910-935)
+ *        -> pc_umeth_3D            (Source/Godunov.cpp:59-476, declared Source/Godunov.H:1142-1162)
+ *   PeleC::estTimeStep hydro part  (Source/PeleC.cpp:829-960, Source/Timestep.H:51-88)
+ *   construct_Snew + computeTemp   (Source/Advance.cpp:397-417, Source/PeleC.cpp:2289-2305)
+ *
+ * Arrays are described by pcg_array4, which addresses memory exactly like
+ * amrex::Array4<Real>: p[(i-begin[0]) + (j-begin[1])*jstride + (k-begin[2])*kstride
+ * + n*nstride], end[] exclusive. All array pointers are DEVICE pointers unless stated.
+ * Component layouts follow Source/IndexDefines.H (URHO..UTEMP, UFS; QRHO..QTEMP, QFS;
+ * QGAMC..QRSPEC) with NUM_ADV = NUM_AUX = NUM_LIN = 0.
+ *
+ * Every call is asynchronous on the given stream (NULL = legacy default stream) and
+ * returns PCG_OK or a negative PCG_E* code; pcg_last_error() gives the message of the
+ * calling thread's last failure. Nothing aborts the process. Calls are reentrant.
+ */
+#ifndef PCG_HYDRO_H
+#define PCG_HYDRO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* pcg_stream_t; /* same type as cudaStream_t */
+
+enum {
+  PCG_OK = 0,
+  PCG_EINVAL = -1,       /* bad argument (box, array extent, parameter) */
+  PCG_ECUDA = -2,        /* a CUDA runtime call failed */
+  PCG_ENOMEM = -3,       /* device allocation failed */
+  PCG_EUNSUPPORTED = -4, /* option not implemented (e.g. hybrid WENO, inflow BC) */
+  PCG_ETIMEDOUT = -5,    /* a bounded device wait gave up */
+  PCG_EBUDGET = -6,      /* serving: request exceeds the memory budget */
+  PCG_ENOEOS = -7        /* no EOS table set for this species count */
+};
+
+/* Physical boundary types, numbered as PCPhysBCType (Source/PeleC.H:49-57). */
+enum { PCG_BC_INTERIOR = 0, PCG_BC_INFLOW, PCG_BC_OUTFLOW, PCG_BC_SYMMETRY,
+       PCG_BC_SLIP_WALL, PCG_BC_NO_SLIP_WALL, PCG_BC_USER };
+
+/* Arithmetic of the advance. */
+enum {
+  PCG_PREC_FP64 = 0,      /* plain FP64, reference operation order, no FMA contraction */
+  PCG_PREC_FP64_FAST = 1, /* FP64 with FMA contraction */
+  PCG_PREC_MIXED = 2      /* FP32 trace, Riemann and transverse terms; FP64 state,
+                             flux-divergence accumulation, T(e) Newton and dt */
+};
+
+typedef struct pcg_array4 {
+  double* p;
+  int64_t jstride, kstride, nstride;
+  int32_t begin[3], end[3];
+  int32_t ncomp;
+} pcg_array4;
+
+/* Runtime parameters of pc_umdrv / pc_umeth_3D (names and defaults of
+ * Source/Params/_cpp_parameters: difmag 0.1, ppm_type 0, plm_iorder 4,
+ * use_flattening 1, use_hybrid_weno 0). */
+typedef struct pcg_hydro_params {
+  double dx[3];
+  double dt;
+  double difmag;
+  int32_t ppm_type;       /* 0 PLM, 1 PPM */
+  int32_t plm_iorder;     /* 1, 2 or 4 */
+  int32_t use_flattening;
+  int32_t use_hybrid_weno; /* must be 0 */
+  int32_t weno_scheme;
+  int32_t domlo[3], domhi[3];
+  int32_t bclo[3], bchi[3];
+  int32_t nspec;          /* NUM_SPECIES: 1 (gamma law) or 9 (NASA-7 mixture) */
+  int32_t precision_mode; /* PCG_PREC_* */
+} pcg_hydro_params;
+
+/* One box of a batched advance (the body of the MFIter loop, Source/Hydro.cpp:70-288).
+ * uin: conserved state with >= 4 ghost cells; uout: hydro_source on the valid box
+ * (overwritten: the batched call zeroes it first, as Hydro.cpp:47 does);
+ * flx[d]: optional (p == NULL) area-weighted fluxes on the d-faces of the box.
+ * dx, dt, domain and boundary data are per box so that boxes of unrelated runs can
+ * share one launch. */
+typedef struct pcg_box {
+  int32_t lo[3], hi[3];
+  int32_t domlo[3], domhi[3];
+  int32_t bclo[3], bchi[3];
+  double dx[3];
+  double dt;
+  pcg_array4 uin;
+  pcg_array4 uout;
+  pcg_array4 flx[3];
+} pcg_box;
+
+/* ---- set-up --------------------------------------------------------------- */
+
+/* Select the CUDA device for the calling thread's subsequent calls. */
+int pcg_init(int device);
+
+/* EOS tables (PelePhysics' eos(), not in the reference checkout; documented
+ * restatement). Gamma law: one species, constant gamma, molecular weight mw. */
+int pcg_set_eos_gamma(double gamma, double mw);
+/* Ideal-gas mixture with NASA-7 polynomials: a_lo/a_hi hold 7 coefficients per
+ * species (HOST pointers), tmid the range split per species. */
+int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid,
+                      const double* a_lo, const double* a_hi);
+
+const char* pcg_last_error(void);
+
+/* ---- the reference operator surface ---------------------------------------- */
+
+/* pc_ctoprim over [lo,hi] (Source/PeleCUtilities.H:242-320): u -> q (QVAR comps),
+ * qaux (NQAUX comps). Replaces the launch at Source/Hydro.cpp:104-116. */
+int pcg_ctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+                const pcg_array4* u, pcg_array4* q, pcg_array4* qaux, pcg_stream_t stream);
+
+/* pc_umdrv (Source/Hydro.H:910-935). q, qaux, src_q must cover grow(bx,4); src_q may
+ * be NULL (no sources). uout is accumulated into (uout += hydro source), flx[3] is
+ * overwritten with area-weighted fluxes, area[3]/vol are the geometry FABs.
+ * Replaces Source/Hydro.cpp:245-249. */
+int pcg_umdrv(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+              const pcg_array4* uin, pcg_array4* uout, const pcg_array4* q,
+              const pcg_array4* qaux, const pcg_array4* src_q, pcg_array4* flx,
+              const pcg_array4* area, const pcg_array4* vol, pcg_stream_t stream);
+
+/* One construct_hydro_source box iteration (Source/Hydro.cpp:70-249 for a regular
+ * box, no sources): ctoprim on grow(bx,4), then pc_umdrv. uout is zeroed first;
+ * flx may be NULL. Geometry is uniform Cartesian from prm->dx. */
+int pcg_hydro_box(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+                  const pcg_array4* uin, pcg_array4* uout, pcg_array4* flx,
+                  pcg_stream_t stream);
+
+/* ---- batched form -------------------------------------------------------------- */
+
+/* construct_hydro_source over many boxes in one set of launches: every box of the
+ * list is advanced by its own dx/dt/domain/BCs; ppm_type, plm_iorder,
+ * use_flattening, difmag, nspec and precision_mode come from prm (its dx, dt, dom*,
+ * bc* are ignored). Uniform Cartesian geometry. */
+int pcg_hydro_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes,
+                    pcg_stream_t stream);
+
+/* pc_estdt_hydro over the valid cells of every box (Source/Timestep.H:51-88), the
+ * min over boxes, times cfl (Source/PeleC.cpp:930). dt_out is a DEVICE pointer
+ * to one double, written asynchronously. Each box's dx is used. */
+int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl,
+              double* dt_out, pcg_stream_t stream);
+
+/* construct_Snew (S_new = S_old + dt*hydro_source, Source/Advance.cpp:397-417) and
+ * computeTemp (Source/PeleC.cpp:2289-2305: pc_rst_int_e default branch, then the
+ * T(e) Newton of pc_cmpTemp) on the valid cells of every box: reads boxes[b].uin as
+ * S_old and boxes[b].uout as hydro_source, writes S_new into s_new[b]. dt is a
+ * DEVICE pointer (NULL: each box's dt). s_new may alias uin. */
+int pcg_update_state(int32_t nspec, int32_t nbox, const pcg_box* boxes,
+                     const pcg_array4* s_new, const double* dt, pcg_stream_t stream);
+
+/* Single-level ghost fill of a domain-sized FAB covering grow(domain, ng): periodic
+ * wrap in periodic directions, zero-gradient extrapolation (foextrap) otherwise.
+ * The FillBoundary/FillPatch step that precedes the advance (Source/Advance.cpp:307-309). */
+int pcg_fill_ghosts(const pcg_array4* state, const int32_t domlo[3], const int32_t domhi[3],
+                    const int32_t periodic[3], int32_t ng, pcg_stream_t stream);
+
+/* ---- persistent plans (repeated steps, CUDA-graph capture) -------------------- */
+
+/* A plan fixes a box list and owns its workspace and launch tables, so that its run
+ * functions allocate nothing and can be captured in a CUDA graph. It replaces the
+ * per-step box loop of construct_hydro_source (Source/Hydro.cpp:70-288) plus the
+ * estTimeStep reduction and the state update of the level advance.
+ * fuse != 0 lets the plan advance boxes that tile one shared state array as their
+ * bounding box (bit-identical results, no repeated halo work). */
+typedef struct pcg_plan pcg_plan;
+int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes,
+                    int32_t fuse, pcg_plan** plan);
+/* construct_hydro_source over the plan's boxes; dt_dev: DEVICE pointer to the step's
+ * dt, or NULL to use each box's dt. */
+int pcg_plan_hydro(pcg_plan* plan, const double* dt_dev, pcg_stream_t stream);
+/* cfl * min over the plan's boxes of pc_estdt_hydro, into *dt_dev (DEVICE). */
+int pcg_plan_estdt(pcg_plan* plan, double cfl, double* dt_dev, pcg_stream_t stream);
+/* S_new = S_old + dt * hydro_source in place in each box's uin, then computeTemp. */
+int pcg_plan_update(pcg_plan* plan, const double* dt_dev, pcg_stream_t stream);
+int pcg_plan_info(const pcg_plan* plan, int64_t* workspace_bytes, int32_t* nregions,
+                  int64_t* blocks_per_stage /* [7] */);
+int pcg_plan_destroy(pcg_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

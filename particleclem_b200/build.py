@@ -1,0 +1,79 @@
+"""Build the CUDA library in-tree: particleclem_b200/_lib/libpcg_hydro.so.
+
+Three translation units, all for sm_100a:
+  pcg_kernels_strict.cu  FP64 kernels, --fmad=false (reference rounding, operation by operation)
+  pcg_kernels_fast.cu    FP64 with FMA contraction, and the mixed FP32/FP64 kernels
+  pcg_host.cu            host runtime and the C ABI of include/pcg_hydro.h
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libpcg_hydro.so")
+ROOT = os.path.dirname(HERE)
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+          "-I", SRC, "-I", os.path.join(ROOT, "include")]
+UNITS = {
+    "pcg_kernels_strict.cu": ["--fmad=false"],
+    "pcg_kernels_fast.cu": ["--fmad=true"],
+    "pcg_host.cu": [],
+}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _sources_mtime() -> float:
+    paths = [os.path.join(SRC, f) for f in os.listdir(SRC)] + [os.path.join(ROOT, "include", "pcg_hydro.h")]
+    return max(os.path.getmtime(p) for p in paths)
+
+
+def up_to_date() -> bool:
+    return os.path.exists(LIB) and os.path.getmtime(LIB) >= _sources_mtime()
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    cc = nvcc()
+
+    def compile_unit(item):
+        src, extra = item
+        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
+        cmd = [cc, *COMMON, *ARCH, *extra, "-c", os.path.join(SRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+        objs = list(ex.map(compile_unit, UNITS.items()))
+    tmp = LIB + ".tmp"
+    cmd = [cc, "-shared", *ARCH, "-o", tmp, *objs, "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB)
+    for o in objs:
+        os.remove(o)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,160 @@
+// pcg_aux_kernels.cuh -- the steps either side of the advance: the CFL timestep
+// reduction, the state update with the temperature Newton solve, and the single-level
+// ghost fill. All FP64.
+#pragma once
+
+#include "pcg_device.cuh"
+
+namespace PCG_TU {
+
+enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL };
+
+__device__ __forceinline__ bool aux_item(const pcg::AuxArgs& a, const pcg::AuxBox*& bx, int& i, int& j, int& k) {
+  const int64_t blk = blockIdx.x;
+  int lo = 0, hi = a.nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.segs[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
+  }
+  const pcg::Seg& s = a.segs[lo];
+  const int64_t local = (blk - s.blk0) * blockDim.x + threadIdx.x;
+  if (local >= s.count) return false;
+  const int64_t t = local / s.n[0];
+  i = s.lo[0] + (int)(local - t * s.n[0]);
+  j = s.lo[1] + (int)(t % s.n[1]);
+  k = s.lo[2] + (int)(t / s.n[1]);
+  bx = a.boxes + s.region;
+  return true;
+}
+
+// Block minimum with warp shuffles (blockDim.x == 128).
+__device__ __forceinline__ double block_min(double v) {
+  __shared__ double sh[4];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = (threadIdx.x < 4) ? sh[threadIdx.x] : DBL_MAX;
+#pragma unroll
+    for (int o = 2; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+
+// Source/Timestep.H:51-88 (pc_estdt_hydro): per-cell dx_d / (c + |u_d|), block minima.
+template <int NS, bool MIX>
+__global__ void __launch_bounds__(128) k_estdt(pcg::AuxArgs a) {
+  const pcg::AuxBox* bx;
+  int i, j, k;
+  double dt = DBL_MAX;
+  if (aux_item(a, bx, i, j, k)) {
+    using E = Eos<NS, MIX, double>;
+    const V4<const double> u = v4<const double>(bx->uin);
+    const double rho = u(i, j, k, pcg::URHO);
+    const double rhoInv = 1.0 / rho;
+    const double T = u(i, j, k, pcg::UTEMP);
+    double y[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) y[n] = u(i, j, k, pcg::UFS + n) * rhoInv;
+    const double c = E::rty2cs(rho, T, y);
+    const double ux = u(i, j, k, pcg::UMX) * rhoInv;
+    dt = dmin(dt, bx->dx[0] / (c + fabs(ux)));
+    const double uy = u(i, j, k, pcg::UMY) * rhoInv;
+    dt = dmin(dt, bx->dx[1] / (c + fabs(uy)));
+    const double uz = u(i, j, k, pcg::UMZ) * rhoInv;
+    dt = dmin(dt, bx->dx[2] / (c + fabs(uz)));
+  }
+  dt = block_min(dt);
+  if (threadIdx.x == 0) a.partial[blockIdx.x] = dt;
+}
+
+// Final reduction of the block minima, then estdt_hydro *= cfl (Source/PeleC.cpp:930).
+__global__ void __launch_bounds__(128) k_estdt_final(pcg::AuxArgs a) {
+  double v = DBL_MAX;
+  for (int64_t b = threadIdx.x; b < a.npartial; b += blockDim.x) v = dmin(v, a.partial[b]);
+  v = block_min(v);
+  if (threadIdx.x == 0) *a.dt_out = v * a.cfl;
+}
+
+// Source/Advance.cpp:397-417 (construct_Snew, hydro only) then Source/PeleC.cpp:2289-2305
+// (computeTemp): pc_rst_int_e default branch (PeleCUtilities.H:227-235) and pc_cmpTemp
+// (PeleCUtilities.H:70-84).
+template <int NS, bool MIX>
+__global__ void __launch_bounds__(128) k_update(pcg::AuxArgs a) {
+  const pcg::AuxBox* bx;
+  int i, j, k;
+  if (!aux_item(a, bx, i, j, k)) return;
+  using E = Eos<NS, MIX, double>;
+  const double dt = a.dt_in ? *a.dt_in : bx->dt;
+  const V4<const double> so = v4<const double>(bx->uin);
+  const V4<const double> hs = v4<const double>(bx->uout);
+  const V4<double> sn = v4<double>(bx->snew);
+  double s[pcg::nvar(NS)];
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) {
+    s[n] = so(i, j, k, n);
+    s[n] += dt * hs(i, j, k, n);
+  }
+  const double rho = s[pcg::URHO];
+  const double rhoInv = 1.0 / rho;
+  const double Up = s[pcg::UMX] * rhoInv;
+  const double Vp = s[pcg::UMY] * rhoInv;
+  const double Wp = s[pcg::UMZ] * rhoInv;
+  const double ke = 0.5 * (Up * Up + Vp * Vp + Wp * Wp) - 0.5 * 0.0 * 0.0 * 0.0 * 0.0;
+  s[pcg::UEINT] = s[pcg::UEDEN] - rho * ke;
+  const double rhoInv2 = 1.0 / s[pcg::URHO];
+  const double e = s[pcg::UEINT] * rhoInv2;
+  double y[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) y[n] = s[pcg::UFS + n] * rhoInv2;
+  s[pcg::UTEMP] = E::rey2t(e, y, s[pcg::UTEMP]);
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) sn(i, j, k, n) = s[n];
+}
+
+// Single-level FillBoundary of one direction: the ghost slabs of a domain FAB that
+// covers grow(domain, ng), full extent in the other two directions (so corners are
+// filled consistently when the directions run x, y, z in turn).
+__global__ void __launch_bounds__(128) k_fill(pcg::AuxArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int d = a.dir, ng = a.ng;
+  int ext[3];
+  for (int e = 0; e < 3; ++e) ext[e] = a.dhi[e] - a.dlo[e] + 1 + 2 * ng;
+  ext[d] = 2 * ng;  // ghost layers of direction d only
+  const int64_t ncell = (int64_t)ext[0] * ext[1] * ext[2];
+  if (t >= ncell) return;
+  int c[3];
+  c[0] = (int)(t % ext[0]);
+  c[1] = (int)((t / ext[0]) % ext[1]);
+  c[2] = (int)(t / ((int64_t)ext[0] * ext[1]));
+  int dst[3], src[3];
+  for (int e = 0; e < 3; ++e) dst[e] = a.dlo[e] - ng + c[e];
+  const int n = a.dhi[d] - a.dlo[d] + 1;
+  const int g = c[d];  // 0..ng-1 low side, ng..2ng-1 high side
+  dst[d] = (g < ng) ? a.dlo[d] - ng + g : a.dhi[d] + 1 + (g - ng);
+  for (int e = 0; e < 3; ++e) src[e] = dst[e];
+  if (a.periodic) {
+    src[d] = (g < ng) ? dst[d] + n : dst[d] - n;
+  } else {
+    src[d] = (g < ng) ? a.dlo[d] : a.dhi[d];
+  }
+  const V4<double> s = v4<double>(a.state);
+  for (int comp = 0; comp < a.ncomp; ++comp) s(dst[0], dst[1], dst[2], comp) = s(src[0], src[1], src[2], comp);
+}
+
+template <int NS, bool MIX>
+static cudaError_t launch_aux_t(int which, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s) {
+  if (nblocks <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)nblocks), block(128);
+  switch (which) {
+    case AUX_ESTDT: k_estdt<NS, MIX><<<grid, block, 0, s>>>(a); break;
+    case AUX_ESTDT_FINAL: k_estdt_final<<<1, block, 0, s>>>(a); break;
+    case AUX_UPDATE: k_update<NS, MIX><<<grid, block, 0, s>>>(a); break;
+    case AUX_FILL: k_fill<<<grid, block, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace PCG_TU

@@ -1,0 +1,950 @@
+// pcg_host.cu -- host runtime behind include/pcg_hydro.h: argument checks, EOS
+// tables, workspace layout, launch plans and the C entry points.
+//
+// A launch plan lays out, for every box (region) of a call, the intermediate arrays
+// of the advance in one device workspace and builds per-stage segment tables (see
+// pcg_types.h). One-shot calls allocate the workspace stream-ordered
+// (cudaMallocAsync / cudaFreeAsync on the caller's stream, the role
+// amrex::The_Async_Arena plays in the reference); pcg_plan objects keep it for
+// repeated steps so that a step can be captured in a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pcg_hydro.h"
+#include "pcg_types.h"
+
+namespace pcg_strict {
+cudaError_t upload_eos(int slot, const pcg::EosConst& e);
+cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, cudaStream_t s);
+cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
+}  // namespace pcg_strict
+namespace pcg_fast {
+cudaError_t upload_eos(int slot, const pcg::EosConst& e);
+cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, cudaStream_t s);
+cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
+}  // namespace pcg_fast
+
+namespace {
+
+enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
+enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL };
+constexpr int kThreads = 128;
+constexpr size_t kAlign = 256;
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      cudaGetLastError();                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? PCG_ENOMEM : PCG_ECUDA, "%s: %s", #call, \
+                  cudaGetErrorString(e_));                                              \
+    }                                                                                   \
+  } while (0)
+
+// ------------------------------------------------------------------ EOS tables
+struct EosState {
+  std::mutex mu;
+  bool set[2] = {false, false};
+  pcg::EosConst c[2];
+  uint64_t version[2] = {0, 0};
+  uint64_t uploaded[64][2] = {};  // per device
+};
+EosState& eos_state() {
+  static EosState s;
+  return s;
+}
+
+int eos_slot(int nspec) { return nspec == 1 ? 0 : 1; }
+
+int ensure_eos(int nspec) {
+  EosState& es = eos_state();
+  const int slot = eos_slot(nspec);
+  std::lock_guard<std::mutex> lk(es.mu);
+  if (!es.set[slot] || es.c[slot].nspec != nspec)
+    return fail(PCG_ENOEOS, "no EOS table set for nspec=%d (pcg_set_eos_gamma / pcg_set_eos_nasa7)", nspec);
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(PCG_EINVAL, "device index %d out of range", dev);
+  if (es.uploaded[dev][slot] != es.version[slot]) {
+    CUDA_TRY(pcg_strict::upload_eos(slot, es.c[slot]));
+    CUDA_TRY(pcg_fast::upload_eos(slot, es.c[slot]));
+    es.uploaded[dev][slot] = es.version[slot];
+  }
+  return PCG_OK;
+}
+
+int store_eos(int slot, const pcg::EosConst& c) {
+  EosState& es = eos_state();
+  {
+    std::lock_guard<std::mutex> lk(es.mu);
+    es.c[slot] = c;
+    es.set[slot] = true;
+    es.version[slot] += 1;
+  }
+  return ensure_eos(c.nspec);
+}
+
+// ------------------------------------------------------------------ boxes & views
+struct IBox {
+  int lo[3], hi[3];
+  int64_t n(int d) const { return hi[d] - lo[d] + 1; }
+  int64_t cells() const { return n(0) * n(1) * n(2); }
+  bool ok() const { return hi[0] >= lo[0] && hi[1] >= lo[1] && hi[2] >= lo[2]; }
+};
+IBox mkbox(const int32_t* lo, const int32_t* hi) {
+  IBox b;
+  for (int d = 0; d < 3; ++d) { b.lo[d] = lo[d]; b.hi[d] = hi[d]; }
+  return b;
+}
+IBox grow(IBox b, int n) {
+  for (int d = 0; d < 3; ++d) { b.lo[d] -= n; b.hi[d] += n; }
+  return b;
+}
+IBox grow_dir(IBox b, int d, int n) { b.lo[d] -= n; b.hi[d] += n; return b; }
+IBox nodes(IBox b, int d) { b.hi[d] += 1; return b; }
+
+pcg::View view_of(const pcg_array4* a) {
+  pcg::View v{};
+  if (!a || !a->p) return v;
+  v.p = a->p;
+  v.js = a->jstride;
+  v.ks = a->kstride;
+  v.ns = a->nstride;
+  for (int d = 0; d < 3; ++d) v.b[d] = a->begin[d];
+  return v;
+}
+
+bool covers(const pcg_array4* a, const IBox& b, int ncomp) {
+  if (!a || !a->p) return false;
+  for (int d = 0; d < 3; ++d)
+    if (a->begin[d] > b.lo[d] || a->end[d] <= b.hi[d]) return false;
+  return a->ncomp >= ncomp;
+}
+
+int check_array(const char* what, const pcg_array4* a, const IBox& b, int ncomp) {
+  if (!covers(a, b, ncomp))
+    return fail(PCG_EINVAL, "%s must cover [%d,%d,%d]-[%d,%d,%d] with %d components", what, b.lo[0], b.lo[1],
+                b.lo[2], b.hi[0], b.hi[1], b.hi[2], ncomp);
+  return PCG_OK;
+}
+
+int check_params(const pcg_hydro_params* p) {
+  if (!p) return fail(PCG_EINVAL, "params is NULL");
+  if (p->nspec != 1 && p->nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d: kernels exist for 1 and 9", p->nspec);
+  if (p->ppm_type != 0 && p->ppm_type != 1) return fail(PCG_EINVAL, "PeleC::ppm_type must be 0 (PLM) or 1 (PPM)");
+  if (p->use_hybrid_weno) return fail(PCG_EUNSUPPORTED, "hybrid WENO reconstruction is not implemented");
+  if (p->ppm_type == 0 && p->plm_iorder != 1 && p->plm_iorder != 2 && p->plm_iorder != 4)
+    return fail(PCG_EINVAL, "plm_iorder must be 1, 2 or 4");
+  if (p->precision_mode < PCG_PREC_FP64 || p->precision_mode > PCG_PREC_MIXED)
+    return fail(PCG_EINVAL, "precision_mode %d", p->precision_mode);
+  return PCG_OK;
+}
+
+int check_box_common(const IBox& bx, const double* dx, double dt, const int32_t* bclo, const int32_t* bchi) {
+  if (!bx.ok()) return fail(PCG_EINVAL, "empty box");
+  for (int d = 0; d < 3; ++d) {
+    if (!(dx[d] > 0.0) || !std::isfinite(dx[d])) return fail(PCG_EINVAL, "dx[%d] must be positive", d);
+    if (bclo[d] == PCG_BC_INFLOW || bclo[d] == PCG_BC_USER || bchi[d] == PCG_BC_INFLOW || bchi[d] == PCG_BC_USER)
+      return fail(PCG_EUNSUPPORTED, "inflow/user_bc boundaries (pc_low_order_boundary) are not implemented");
+  }
+  if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(PCG_EINVAL, "dt must be finite and >= 0");
+  return PCG_OK;
+}
+
+// ------------------------------------------------------------------ launch plans
+struct BoxIn {
+  IBox bx;
+  int domlo[3], domhi[3], bclo[3], bchi[3];
+  double dx[3];
+  double dt;
+  pcg::View uin, uout, q, qa, srcq, area[3], vol, flx[3];
+  bool internal_q;  // ctoprim into the workspace
+  bool zero_uout;
+};
+
+struct Layout {
+  int ns = 1;
+  size_t esz = 8;  // compute-type size of the intermediates
+  size_t ws_bytes = 0;
+  std::vector<pcg::Region> regions;
+  std::vector<pcg::Seg> segs[K_NSTAGE];
+  int64_t nblocks[K_NSTAGE] = {};
+};
+
+size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v) {
+  const size_t off = (L.ws_bytes + kAlign - 1) / kAlign * kAlign;
+  v.p = reinterpret_cast<void*>(off);  // rebased once the workspace exists
+  v.js = b.n(0);
+  v.ks = b.n(0) * b.n(1);
+  v.ns = b.cells();
+  for (int d = 0; d < 3; ++d) v.b[d] = b.lo[d];
+  L.ws_bytes = off + size_t(b.cells()) * nc * esz;
+  return off;
+}
+
+void add_seg(Layout& L, int stage, int region, int variant, const IBox& b) {
+  pcg::Seg s{};
+  s.region = region;
+  s.variant = variant;
+  for (int d = 0; d < 3; ++d) { s.lo[d] = b.lo[d]; s.n[d] = (int)b.n(d); }
+  s.count = b.cells();
+  s.blk0 = L.nblocks[stage];
+  L.segs[stage].push_back(s);
+  L.nblocks[stage] += (s.count + kThreads - 1) / kThreads;
+}
+
+void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool single) {
+  L.ns = ns;
+  L.esz = single ? 4 : 8;
+  const int nt = pcg::nt_comps(ns), nf = pcg::nf_comps(ns), nv = pcg::nvar(ns), nq = pcg::qvar(ns);
+  for (size_t r = 0; r < boxes.size(); ++r) {
+    const BoxIn& B = boxes[r];
+    pcg::Region R{};
+    for (int d = 0; d < 3; ++d) {
+      R.lo[d] = B.bx.lo[d];
+      R.hi[d] = B.bx.hi[d];
+      R.domlo[d] = B.domlo[d];
+      R.domhi[d] = B.domhi[d];
+      R.bclo[d] = B.bclo[d];
+      R.bchi[d] = B.bchi[d];
+      R.dx[d] = B.dx[d];
+    }
+    R.dt = B.dt;
+    R.area_u[0] = B.dx[1] * B.dx[2];
+    R.area_u[1] = B.dx[0] * B.dx[2];
+    R.area_u[2] = B.dx[0] * B.dx[1];
+    R.vol_u = B.dx[0] * B.dx[1] * B.dx[2];
+    R.uin = B.uin;
+    R.uout = B.uout;
+    R.srcq = B.srcq;
+    R.vol = B.vol;
+    for (int d = 0; d < 3; ++d) R.area[d] = B.area[d];
+    R.zero_uout = B.zero_uout ? 1 : 0;
+    const IBox g4 = grow(B.bx, 4), g1 = grow(B.bx, 1);
+    if (B.internal_q) {
+      take(L, g4, nq, 8, R.q);
+      take(L, g4, pcg::NQAUX, 8, R.qa);
+      add_seg(L, K_CTOPRIM, (int)r, 0, g4);
+    } else {
+      R.q = B.q;
+      R.qa = B.qa;
+    }
+    take(L, g1, 2, L.esz, R.prep);
+    add_seg(L, K_PREP, (int)r, 0, g1);
+    take(L, nodes(nodes(nodes(B.bx, 0), 1), 2), 1, 8, R.divu);
+    for (int d = 0; d < 3; ++d) {
+      IBox tb = g1;
+      tb.hi[d] += 1;  // d-faces lo-1 .. hi+2
+      take(L, tb, nt, L.esz, R.trm[d]);
+      take(L, tb, nt, L.esz, R.trp[d]);
+      add_seg(L, K_TRACE, (int)r, d, g1);
+    }
+    for (int d = 0; d < 3; ++d) {
+      IBox fb = nodes(grow_dir(g1, d, -1), d);  // d-faces lo..hi+1, others grown by 1
+      take(L, fb, nf, L.esz, R.fi[d]);
+      add_seg(L, K_FLUX0, (int)r, d, fb);
+    }
+    for (int d = 0; d < 3; ++d) {
+      for (int o = 0; o < 3; ++o) {
+        if (o == d) continue;
+        const int t = 3 - d - o;
+        IBox b = nodes(B.bx, d);
+        b = grow_dir(b, t, 1);
+        take(L, b, nf, L.esz, R.fdo[d][o]);
+      }
+      // one thread per d-face computes both (d|o) pairs that reach it
+      add_seg(L, K_FLUX1, (int)r, d, nodes(grow_dir(g1, d, -1), d));
+    }
+    for (int d = 0; d < 3; ++d) {
+      const IBox fb = nodes(B.bx, d);
+      if (B.flx[d].p) {
+        R.ff[d] = B.flx[d];
+      } else {
+        take(L, fb, nv, 8, R.ff[d]);
+      }
+      take(L, fb, 2, 8, R.qec[d]);
+      add_seg(L, K_FLUX2, (int)r, d, fb);
+    }
+    add_seg(L, K_CONSUP, (int)r, 0, B.bx);
+    L.regions.push_back(R);
+  }
+}
+
+void rebase(pcg::View& v, char* base) {
+  v.p = base + reinterpret_cast<size_t>(v.p);
+}
+
+void rebase_workspace(Layout& L, const std::vector<BoxIn>& boxes, char* base) {
+  for (size_t r = 0; r < L.regions.size(); ++r) {
+    pcg::Region& R = L.regions[r];
+    const BoxIn& B = boxes[r];
+    if (B.internal_q) { rebase(R.q, base); rebase(R.qa, base); }
+    rebase(R.prep, base);
+    rebase(R.divu, base);
+    for (int d = 0; d < 3; ++d) {
+      rebase(R.trm[d], base);
+      rebase(R.trp[d], base);
+      rebase(R.fi[d], base);
+      for (int o = 0; o < 3; ++o)
+        if (o != d) rebase(R.fdo[d][o], base);
+      if (!B.flx[d].p) rebase(R.ff[d], base);
+      rebase(R.qec[d], base);
+    }
+  }
+}
+
+// Device copy of the region and segment tables.
+struct Tables {
+  void* dev = nullptr;
+  size_t bytes = 0;
+  const pcg::Region* regions = nullptr;
+  const pcg::Seg* segs[K_NSTAGE] = {};
+  std::vector<char> host;
+};
+
+void pack_tables(const Layout& L, Tables& T) {
+  size_t off = L.regions.size() * sizeof(pcg::Region);
+  size_t seg_off[K_NSTAGE];
+  for (int s = 0; s < K_NSTAGE; ++s) {
+    off = (off + 15) / 16 * 16;
+    seg_off[s] = off;
+    off += L.segs[s].size() * sizeof(pcg::Seg);
+  }
+  T.bytes = std::max<size_t>(off, 16);
+  T.host.assign(T.bytes, 0);
+  if (!L.regions.empty()) std::memcpy(T.host.data(), L.regions.data(), L.regions.size() * sizeof(pcg::Region));
+  for (int s = 0; s < K_NSTAGE; ++s)
+    if (!L.segs[s].empty()) std::memcpy(T.host.data() + seg_off[s], L.segs[s].data(), L.segs[s].size() * sizeof(pcg::Seg));
+  // device pointers are filled in by bind_tables once T.dev exists
+  for (int s = 0; s < K_NSTAGE; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(seg_off[s]);
+}
+
+void bind_tables(Tables& T) {
+  char* base = static_cast<char*>(T.dev);
+  T.regions = reinterpret_cast<const pcg::Region*>(base);
+  for (int s = 0; s < K_NSTAGE; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(base + reinterpret_cast<size_t>(T.segs[s]));
+}
+
+int launch_stages(const Layout& L, const Tables& T, const pcg_hydro_params* p, int first, int last,
+                  const double* dt_dev, cudaStream_t s) {
+  const bool single = p->precision_mode == PCG_PREC_MIXED;
+  for (int st = first; st <= last; ++st) {
+    if (L.nblocks[st] == 0) continue;
+    pcg::StageArgs a{};
+    a.regions = T.regions;
+    a.segs = T.segs[st];
+    a.nseg = (int32_t)L.segs[st].size();
+    a.ppm_type = p->ppm_type;
+    a.plm_iorder = p->plm_iorder;
+    a.use_flattening = p->use_flattening;
+    a.difmag = p->difmag;
+    a.dt_dev = dt_dev;
+    cudaError_t e = (p->precision_mode == PCG_PREC_FP64)
+                      ? pcg_strict::launch_stage(st, L.ns, false, a, L.nblocks[st], s)
+                      : pcg_fast::launch_stage(st, L.ns, single, a, L.nblocks[st], s);
+    if (e != cudaSuccess) return fail(PCG_ECUDA, "stage %d launch: %s", st, cudaGetErrorString(e));
+  }
+  return PCG_OK;
+}
+
+// One-shot execution: stream-ordered workspace and tables, launches, stream-ordered free.
+int run_once(const pcg_hydro_params* p, std::vector<BoxIn>& boxes, int first, int last, cudaStream_t s) {
+  int rc = ensure_eos(p->nspec);
+  if (rc) return rc;
+  Layout L;
+  build_layout(L, boxes, p->nspec, p->precision_mode == PCG_PREC_MIXED);
+  void* ws = nullptr;
+  if (L.ws_bytes) CUDA_TRY(cudaMallocAsync(&ws, L.ws_bytes, s));
+  rebase_workspace(L, boxes, static_cast<char*>(ws));
+  Tables T;
+  pack_tables(L, T);
+  cudaError_t e = cudaMallocAsync(&T.dev, T.bytes, s);
+  if (e != cudaSuccess) {
+    if (ws) cudaFreeAsync(ws, s);
+    cudaGetLastError();
+    return fail(PCG_ENOMEM, "table allocation: %s", cudaGetErrorString(e));
+  }
+  // pageable source: the copy is staged before the call returns
+  e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    bind_tables(T);
+    rc = launch_stages(L, T, p, first, last, nullptr, s);
+  } else {
+    rc = fail(PCG_ECUDA, "table upload: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(T.dev, s);
+  if (ws) cudaFreeAsync(ws, s);
+  return rc;
+}
+
+int box_from_params(const pcg_hydro_params* p, const int32_t* lo, const int32_t* hi, BoxIn& B) {
+  B = BoxIn{};
+  B.bx = mkbox(lo, hi);
+  for (int d = 0; d < 3; ++d) {
+    B.domlo[d] = p->domlo[d];
+    B.domhi[d] = p->domhi[d];
+    B.bclo[d] = p->bclo[d];
+    B.bchi[d] = p->bchi[d];
+    B.dx[d] = p->dx[d];
+  }
+  B.dt = p->dt;
+  return check_box_common(B.bx, B.dx, B.dt, B.bclo, B.bchi);
+}
+
+int box_from_desc(const pcg_box& b, int nv, BoxIn& B) {
+  B = BoxIn{};
+  B.bx = mkbox(b.lo, b.hi);
+  for (int d = 0; d < 3; ++d) {
+    B.domlo[d] = b.domlo[d];
+    B.domhi[d] = b.domhi[d];
+    B.bclo[d] = b.bclo[d];
+    B.bchi[d] = b.bchi[d];
+    B.dx[d] = b.dx[d];
+  }
+  B.dt = b.dt;
+  int rc = check_box_common(B.bx, B.dx, B.dt, B.bclo, B.bchi);
+  if (rc) return rc;
+  if ((rc = check_array("box uin", &b.uin, grow(B.bx, 4), nv))) return rc;
+  if ((rc = check_array("box uout", &b.uout, B.bx, nv))) return rc;
+  B.uin = view_of(&b.uin);
+  B.uout = view_of(&b.uout);
+  for (int d = 0; d < 3; ++d) {
+    if (b.flx[d].p) {
+      if ((rc = check_array("box flx", &b.flx[d], nodes(B.bx, d), nv))) return rc;
+      B.flx[d] = view_of(&b.flx[d]);
+    }
+  }
+  B.internal_q = true;
+  B.zero_uout = true;
+  return PCG_OK;
+}
+
+// Merge boxes that tile one shared array into their bounding box. Every output of the
+// advance depends only on traced states in grow(box,1), whose flattening stencil
+// (+-3) always lies inside the grow(box,4) FAB, so the result of a box does not
+// depend on how its level is cut into boxes; a merged region gives bit-identical
+// hydro sources and skips the halo work the separate boxes would repeat.
+void fuse_boxes(std::vector<BoxIn>& boxes) {
+  std::vector<bool> used(boxes.size(), false);
+  std::vector<BoxIn> out;
+  for (size_t a = 0; a < boxes.size(); ++a) {
+    if (used[a]) continue;
+    std::vector<size_t> grp{a};
+    used[a] = true;
+    const BoxIn& A = boxes[a];
+    bool mergeable = !A.flx[0].p && !A.flx[1].p && !A.flx[2].p;
+    for (size_t b = a + 1; mergeable && b < boxes.size(); ++b) {
+      const BoxIn& B = boxes[b];
+      if (used[b] || B.flx[0].p || B.flx[1].p || B.flx[2].p) continue;
+      if (B.uin.p != A.uin.p || B.uout.p != A.uout.p || B.uin.js != A.uin.js || B.uin.ks != A.uin.ks ||
+          B.uout.js != A.uout.js || B.uout.ks != A.uout.ks || B.dt != A.dt)
+        continue;
+      bool same = true;
+      for (int d = 0; d < 3; ++d)
+        same = same && B.dx[d] == A.dx[d] && B.domlo[d] == A.domlo[d] && B.domhi[d] == A.domhi[d] &&
+               B.bclo[d] == A.bclo[d] && B.bchi[d] == A.bchi[d] && B.uin.b[d] == A.uin.b[d] &&
+               B.uout.b[d] == A.uout.b[d];
+      if (!same) continue;
+      grp.push_back(b);
+    }
+    IBox bb = A.bx;
+    int64_t vol = 0;
+    for (size_t g : grp) {
+      for (int d = 0; d < 3; ++d) {
+        bb.lo[d] = std::min(bb.lo[d], boxes[g].bx.lo[d]);
+        bb.hi[d] = std::max(bb.hi[d], boxes[g].bx.hi[d]);
+      }
+      vol += boxes[g].bx.cells();
+    }
+    bool disjoint = true;
+    for (size_t x = 0; x < grp.size() && disjoint; ++x)
+      for (size_t y = x + 1; y < grp.size() && disjoint; ++y) {
+        const IBox &p = boxes[grp[x]].bx, &q = boxes[grp[y]].bx;
+        bool ov = true;
+        for (int d = 0; d < 3; ++d) ov = ov && p.lo[d] <= q.hi[d] && q.lo[d] <= p.hi[d];
+        disjoint = !ov;
+      }
+    if (grp.size() > 1 && disjoint && vol == bb.cells()) {
+      BoxIn M = A;
+      M.bx = bb;
+      out.push_back(M);
+      for (size_t g : grp) used[g] = true;
+    } else {
+      out.push_back(A);
+      for (size_t g = 1; g < grp.size(); ++g) used[grp[g]] = false;
+    }
+  }
+  boxes.swap(out);
+}
+
+int aux_segments(const std::vector<IBox>& bx, std::vector<pcg::Seg>& segs, int64_t& nblocks) {
+  segs.clear();
+  nblocks = 0;
+  for (size_t r = 0; r < bx.size(); ++r) {
+    pcg::Seg s{};
+    s.region = (int32_t)r;
+    for (int d = 0; d < 3; ++d) { s.lo[d] = bx[r].lo[d]; s.n[d] = (int)bx[r].n(d); }
+    s.count = bx[r].cells();
+    s.blk0 = nblocks;
+    segs.push_back(s);
+    nblocks += (s.count + kThreads - 1) / kThreads;
+  }
+  return PCG_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+struct pcg_plan {
+  pcg_hydro_params prm;
+  std::vector<BoxIn> boxes;
+  Layout L;
+  Tables T;
+  void* ws = nullptr;
+  // auxiliary kernels over the original (unfused) boxes
+  std::vector<pcg::AuxBox> aux;
+  std::vector<pcg::Seg> aux_segs;
+  int64_t aux_blocks = 0;
+  void* aux_dev = nullptr;  // AuxBox[] + Seg[] + partial[]
+  pcg::AuxBox* d_aux = nullptr;
+  pcg::Seg* d_aux_segs = nullptr;
+  double* d_partial = nullptr;
+  int device = 0;
+};
+
+extern "C" {
+
+int pcg_init(int device) {
+  CUDA_TRY(cudaSetDevice(device));
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;  // keep freed workspace cached in the pool
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  cudaGetLastError();
+  return PCG_OK;
+}
+
+const char* pcg_last_error(void) { return g_err.c_str(); }
+
+int pcg_set_eos_gamma(double gamma, double mw) {
+  if (!(gamma > 1.0) || !(mw > 0.0)) return fail(PCG_EINVAL, "gamma must be > 1 and mw > 0");
+  pcg::EosConst c{};
+  c.kind = 0;
+  c.nspec = 1;
+  c.gamma = gamma;
+  c.imw[0] = 1.0 / mw;
+  c.gammaf = (float)gamma;
+  c.imwf[0] = (float)c.imw[0];
+  return store_eos(0, c);
+}
+
+int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid, const double* a_lo, const double* a_hi) {
+  if (nspec < 1 || nspec > pcg::MAXNS) return fail(PCG_EINVAL, "nspec must be in 1..%d", pcg::MAXNS);
+  if (!mw || !tmid || !a_lo || !a_hi) return fail(PCG_EINVAL, "NULL table");
+  pcg::EosConst c{};
+  c.kind = 1;
+  c.nspec = nspec;
+  for (int k = 0; k < nspec; ++k) {
+    if (!(mw[k] > 0.0)) return fail(PCG_EINVAL, "mw[%d] must be > 0", k);
+    const double rw = pcg::RU / mw[k];
+    c.imw[k] = 1.0 / mw[k];
+    c.tmid[k] = tmid[k];
+    for (int r = 0; r < 2; ++r) {
+      const double* a = (r == 0 ? a_lo : a_hi) + 7 * k;
+      c.cvc[k][r][0] = rw * (a[0] - 1.0);
+      c.cvc[k][r][1] = rw * a[1];
+      c.cvc[k][r][2] = rw * a[2];
+      c.cvc[k][r][3] = rw * a[3];
+      c.cvc[k][r][4] = rw * a[4];
+      c.ec[k][r][0] = rw * a[5];
+      c.ec[k][r][1] = rw * (a[0] - 1.0);
+      c.ec[k][r][2] = rw * (a[1] / 2.0);
+      c.ec[k][r][3] = rw * (a[2] / 3.0);
+      c.ec[k][r][4] = rw * (a[3] / 4.0);
+      c.ec[k][r][5] = rw * (a[4] / 5.0);
+      for (int i = 0; i < 5; ++i) c.cvcf[k][r][i] = (float)c.cvc[k][r][i];
+      for (int i = 0; i < 6; ++i) c.ecf[k][r][i] = (float)c.ec[k][r][i];
+    }
+    c.imwf[k] = (float)c.imw[k];
+    c.tmidf[k] = (float)c.tmid[k];
+  }
+  return store_eos(1, c);
+}
+
+int pcg_ctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* u,
+                pcg_array4* q, pcg_array4* qaux, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  const IBox bx = mkbox(lo, hi);
+  if (!bx.ok()) return fail(PCG_EINVAL, "empty box");
+  const int nv = pcg::nvar(prm->nspec), nq = pcg::qvar(prm->nspec);
+  if ((rc = check_array("u", u, bx, nv)) || (rc = check_array("q", q, bx, nq)) ||
+      (rc = check_array("qaux", qaux, bx, pcg::NQAUX)))
+    return rc;
+  if ((rc = ensure_eos(prm->nspec))) return rc;
+  // A one-region plan with only the ctoprim stage, on the caller's arrays.
+  Layout L;
+  L.ns = prm->nspec;
+  pcg::Region R{};
+  R.uin = view_of(u);
+  R.q = view_of(q);
+  R.qa = view_of(qaux);
+  L.regions.push_back(R);
+  add_seg(L, K_CTOPRIM, 0, 0, bx);
+  Tables T;
+  pack_tables(L, T);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMallocAsync(&T.dev, T.bytes, s));
+  cudaError_t e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    bind_tables(T);
+    pcg_hydro_params p = *prm;
+    p.precision_mode = PCG_PREC_FP64;
+    rc = launch_stages(L, T, &p, K_CTOPRIM, K_CTOPRIM, nullptr, s);
+  } else {
+    rc = fail(PCG_ECUDA, "table upload: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(T.dev, s);
+  return rc;
+}
+
+int pcg_umdrv(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* uin,
+              pcg_array4* uout, const pcg_array4* q, const pcg_array4* qaux, const pcg_array4* src_q,
+              pcg_array4* flx, const pcg_array4* area, const pcg_array4* vol, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  std::vector<BoxIn> boxes(1);
+  BoxIn& B = boxes[0];
+  if ((rc = box_from_params(prm, lo, hi, B))) return rc;
+  const int nv = pcg::nvar(prm->nspec), nq = pcg::qvar(prm->nspec);
+  const IBox g4 = grow(B.bx, 4);
+  if ((rc = check_array("uin", uin, grow(B.bx, 1), nv))) return rc;
+  if ((rc = check_array("uout", uout, B.bx, nv))) return rc;
+  if ((rc = check_array("q", q, g4, nq))) return rc;
+  if ((rc = check_array("qaux", qaux, g4, pcg::NQAUX))) return rc;
+  if (src_q && src_q->p && (rc = check_array("src_q", src_q, g4, nq))) return rc;
+  if (!flx || !area || !vol) return fail(PCG_EINVAL, "flx, area and vol are required");
+  for (int d = 0; d < 3; ++d) {
+    if ((rc = check_array("flx", &flx[d], nodes(B.bx, d), nv))) return rc;
+    if ((rc = check_array("area", &area[d], nodes(B.bx, d), 1))) return rc;
+  }
+  if ((rc = check_array("vol", vol, B.bx, 1))) return rc;
+  B.uin = view_of(uin);
+  B.uout = view_of(uout);
+  B.q = view_of(q);
+  B.qa = view_of(qaux);
+  B.srcq = view_of(src_q);
+  B.vol = view_of(vol);
+  for (int d = 0; d < 3; ++d) {
+    B.area[d] = view_of(&area[d]);
+    B.flx[d] = view_of(&flx[d]);
+  }
+  B.internal_q = false;
+  B.zero_uout = false;
+  return run_once(prm, boxes, K_PREP, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pcg_hydro_box(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* uin,
+                  pcg_array4* uout, pcg_array4* flx, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  pcg_box b{};
+  for (int d = 0; d < 3; ++d) {
+    b.lo[d] = lo[d];
+    b.hi[d] = hi[d];
+    b.domlo[d] = prm->domlo[d];
+    b.domhi[d] = prm->domhi[d];
+    b.bclo[d] = prm->bclo[d];
+    b.bchi[d] = prm->bchi[d];
+    b.dx[d] = prm->dx[d];
+  }
+  b.dt = prm->dt;
+  if (!uin || !uout) return fail(PCG_EINVAL, "uin and uout are required");
+  b.uin = *uin;
+  b.uout = *uout;
+  if (flx)
+    for (int d = 0; d < 3; ++d) b.flx[d] = flx[d];
+  std::vector<BoxIn> boxes(1);
+  if ((rc = box_from_desc(b, pcg::nvar(prm->nspec), boxes[0]))) return rc;
+  return run_once(prm, boxes, K_CTOPRIM, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pcg_hydro_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  if (nbox < 0 || (nbox > 0 && !boxes)) return fail(PCG_EINVAL, "bad box list");
+  if (nbox == 0) return PCG_OK;
+  std::vector<BoxIn> bs(nbox);
+  for (int b = 0; b < nbox; ++b)
+    if ((rc = box_from_desc(boxes[b], pcg::nvar(prm->nspec), bs[b]))) return rc;
+  return run_once(prm, bs, K_CTOPRIM, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl, double* dt_out, pcg_stream_t stream) {
+  if (nspec != 1 && nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d", nspec);
+  if (nbox <= 0 || !boxes || !dt_out) return fail(PCG_EINVAL, "bad arguments");
+  int rc = ensure_eos(nspec);
+  if (rc) return rc;
+  std::vector<pcg::AuxBox> ab(nbox);
+  std::vector<IBox> bx(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    bx[b] = mkbox(boxes[b].lo, boxes[b].hi);
+    if ((rc = check_array("uin", &boxes[b].uin, bx[b], pcg::nvar(nspec)))) return rc;
+    ab[b] = pcg::AuxBox{};
+    for (int d = 0; d < 3; ++d) { ab[b].lo[d] = bx[b].lo[d]; ab[b].hi[d] = bx[b].hi[d]; ab[b].dx[d] = boxes[b].dx[d]; }
+    ab[b].uin = view_of(&boxes[b].uin);
+  }
+  std::vector<pcg::Seg> segs;
+  int64_t nblocks = 0;
+  aux_segments(bx, segs, nblocks);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const size_t b1 = nbox * sizeof(pcg::AuxBox), b2 = segs.size() * sizeof(pcg::Seg), b3 = nblocks * sizeof(double);
+  std::vector<char> host(b1 + b2);
+  std::memcpy(host.data(), ab.data(), b1);
+  std::memcpy(host.data() + b1, segs.data(), b2);
+  char* dev = nullptr;
+  CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&dev), b1 + b2 + b3, s));
+  cudaError_t e = cudaMemcpyAsync(dev, host.data(), b1 + b2, cudaMemcpyHostToDevice, s);
+  rc = PCG_OK;
+  if (e == cudaSuccess) {
+    pcg::AuxArgs a{};
+    a.boxes = reinterpret_cast<const pcg::AuxBox*>(dev);
+    a.segs = reinterpret_cast<const pcg::Seg*>(dev + b1);
+    a.nseg = (int32_t)segs.size();
+    a.partial = reinterpret_cast<double*>(dev + b1 + b2);
+    a.npartial = nblocks;
+    a.cfl = cfl;
+    a.dt_out = dt_out;
+    e = pcg_strict::launch_aux(AUX_ESTDT, nspec, a, nblocks, s);
+    if (e == cudaSuccess) e = pcg_strict::launch_aux(AUX_ESTDT_FINAL, nspec, a, 1, s);
+  }
+  if (e != cudaSuccess) rc = fail(PCG_ECUDA, "estdt: %s", cudaGetErrorString(e));
+  cudaFreeAsync(dev, s);
+  return rc;
+}
+
+int pcg_update_state(int32_t nspec, int32_t nbox, const pcg_box* boxes, const pcg_array4* s_new, const double* dt,
+                     pcg_stream_t stream) {
+  if (nspec != 1 && nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d", nspec);
+  if (nbox <= 0 || !boxes || !s_new) return fail(PCG_EINVAL, "bad arguments");
+  int rc = ensure_eos(nspec);
+  if (rc) return rc;
+  const int nv = pcg::nvar(nspec);
+  std::vector<pcg::AuxBox> ab(nbox);
+  std::vector<IBox> bx(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    bx[b] = mkbox(boxes[b].lo, boxes[b].hi);
+    if ((rc = check_array("uin", &boxes[b].uin, bx[b], nv)) || (rc = check_array("uout", &boxes[b].uout, bx[b], nv)) ||
+        (rc = check_array("s_new", &s_new[b], bx[b], nv)))
+      return rc;
+    ab[b] = pcg::AuxBox{};
+    for (int d = 0; d < 3; ++d) { ab[b].lo[d] = bx[b].lo[d]; ab[b].hi[d] = bx[b].hi[d]; ab[b].dx[d] = boxes[b].dx[d]; }
+    ab[b].dt = boxes[b].dt;
+    ab[b].uin = view_of(&boxes[b].uin);
+    ab[b].uout = view_of(&boxes[b].uout);
+    ab[b].snew = view_of(&s_new[b]);
+  }
+  std::vector<pcg::Seg> segs;
+  int64_t nblocks = 0;
+  aux_segments(bx, segs, nblocks);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const size_t b1 = nbox * sizeof(pcg::AuxBox), b2 = segs.size() * sizeof(pcg::Seg);
+  std::vector<char> host(b1 + b2);
+  std::memcpy(host.data(), ab.data(), b1);
+  std::memcpy(host.data() + b1, segs.data(), b2);
+  char* dev = nullptr;
+  CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&dev), b1 + b2, s));
+  cudaError_t e = cudaMemcpyAsync(dev, host.data(), b1 + b2, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    pcg::AuxArgs a{};
+    a.boxes = reinterpret_cast<const pcg::AuxBox*>(dev);
+    a.segs = reinterpret_cast<const pcg::Seg*>(dev + b1);
+    a.nseg = (int32_t)segs.size();
+    a.dt_in = dt;
+    e = pcg_strict::launch_aux(AUX_UPDATE, nspec, a, nblocks, s);
+  }
+  rc = (e == cudaSuccess) ? PCG_OK : fail(PCG_ECUDA, "update: %s", cudaGetErrorString(e));
+  cudaFreeAsync(dev, s);
+  return rc;
+}
+
+int pcg_fill_ghosts(const pcg_array4* state, const int32_t domlo[3], const int32_t domhi[3],
+                    const int32_t periodic[3], int32_t ng, pcg_stream_t stream) {
+  if (!state || !state->p || ng < 0) return fail(PCG_EINVAL, "bad arguments");
+  IBox dom = mkbox(domlo, domhi);
+  if (!dom.ok()) return fail(PCG_EINVAL, "empty domain");
+  int rc = check_array("state", state, grow(dom, ng), 1);
+  if (rc) return rc;
+  for (int d = 0; d < 3; ++d)
+    if (periodic[d] && dom.n(d) < ng) return fail(PCG_EINVAL, "periodic direction %d shorter than ng", d);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  for (int d = 0; d < 3 && ng > 0; ++d) {
+    pcg::AuxArgs a{};
+    a.dir = d;
+    a.state = view_of(state);
+    for (int e = 0; e < 3; ++e) { a.dlo[e] = domlo[e]; a.dhi[e] = domhi[e]; }
+    a.ng = ng;
+    a.periodic = periodic[d] ? 1 : 0;
+    a.ncomp = state->ncomp;
+    int64_t ncell = 2 * (int64_t)ng;
+    for (int e = 0; e < 3; ++e)
+      if (e != d) ncell *= dom.n(e) + 2 * ng;
+    cudaError_t e = pcg_strict::launch_aux(AUX_FILL, 1, a, (ncell + kThreads - 1) / kThreads, s);
+    if (e != cudaSuccess) return fail(PCG_ECUDA, "fill_ghosts: %s", cudaGetErrorString(e));
+  }
+  return PCG_OK;
+}
+
+// ---- persistent plans ---------------------------------------------------------
+
+int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes, int32_t fuse, pcg_plan** out) {
+  if (!out) return fail(PCG_EINVAL, "out is NULL");
+  *out = nullptr;
+  int rc = check_params(prm);
+  if (rc) return rc;
+  if (nbox <= 0 || !boxes) return fail(PCG_EINVAL, "bad box list");
+  if ((rc = ensure_eos(prm->nspec))) return rc;
+  pcg_plan* P = new pcg_plan();
+  P->prm = *prm;
+  cudaGetDevice(&P->device);
+  P->boxes.resize(nbox);
+  for (int b = 0; b < nbox; ++b)
+    if ((rc = box_from_desc(boxes[b], pcg::nvar(prm->nspec), P->boxes[b]))) {
+      delete P;
+      return rc;
+    }
+  // auxiliary tables over the boxes as given
+  std::vector<IBox> bx(nbox);
+  P->aux.resize(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    bx[b] = P->boxes[b].bx;
+    pcg::AuxBox& a = P->aux[b];
+    a = pcg::AuxBox{};
+    for (int d = 0; d < 3; ++d) { a.lo[d] = bx[b].lo[d]; a.hi[d] = bx[b].hi[d]; a.dx[d] = boxes[b].dx[d]; }
+    a.dt = boxes[b].dt;
+    a.uin = view_of(&boxes[b].uin);
+    a.uout = view_of(&boxes[b].uout);
+    a.snew = a.uin;  // in-place state update
+  }
+  aux_segments(bx, P->aux_segs, P->aux_blocks);
+  if (fuse) fuse_boxes(P->boxes);
+  build_layout(P->L, P->boxes, prm->nspec, prm->precision_mode == PCG_PREC_MIXED);
+  cudaError_t e = cudaSuccess;
+  if (P->L.ws_bytes) e = cudaMalloc(&P->ws, P->L.ws_bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete P;
+    return fail(PCG_ENOMEM, "workspace of %zu bytes: %s", P->L.ws_bytes, cudaGetErrorString(e));
+  }
+  rebase_workspace(P->L, P->boxes, static_cast<char*>(P->ws));
+  pack_tables(P->L, P->T);
+  const size_t b1 = P->aux.size() * sizeof(pcg::AuxBox), b2 = P->aux_segs.size() * sizeof(pcg::Seg),
+               b3 = P->aux_blocks * sizeof(double);
+  if ((e = cudaMalloc(&P->T.dev, P->T.bytes)) == cudaSuccess &&
+      (e = cudaMemcpy(P->T.dev, P->T.host.data(), P->T.bytes, cudaMemcpyHostToDevice)) == cudaSuccess &&
+      (e = cudaMalloc(&P->aux_dev, b1 + b2 + b3)) == cudaSuccess) {
+    char* d = static_cast<char*>(P->aux_dev);
+    std::vector<char> host(b1 + b2);
+    std::memcpy(host.data(), P->aux.data(), b1);
+    std::memcpy(host.data() + b1, P->aux_segs.data(), b2);
+    e = cudaMemcpy(d, host.data(), b1 + b2, cudaMemcpyHostToDevice);
+    P->d_aux = reinterpret_cast<pcg::AuxBox*>(d);
+    P->d_aux_segs = reinterpret_cast<pcg::Seg*>(d + b1);
+    P->d_partial = reinterpret_cast<double*>(d + b1 + b2);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (P->ws) cudaFree(P->ws);
+    if (P->T.dev) cudaFree(P->T.dev);
+    if (P->aux_dev) cudaFree(P->aux_dev);
+    delete P;
+    return fail(PCG_ENOMEM, "plan tables: %s", cudaGetErrorString(e));
+  }
+  bind_tables(P->T);
+  *out = P;
+  return PCG_OK;
+}
+
+int pcg_plan_hydro(pcg_plan* P, const double* dt_dev, pcg_stream_t stream) {
+  if (!P) return fail(PCG_EINVAL, "plan is NULL");
+  int rc = ensure_eos(P->prm.nspec);
+  if (rc) return rc;
+  return launch_stages(P->L, P->T, &P->prm, K_CTOPRIM, K_CONSUP, dt_dev, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pcg_plan_estdt(pcg_plan* P, double cfl, double* dt_dev, pcg_stream_t stream) {
+  if (!P || !dt_dev) return fail(PCG_EINVAL, "bad arguments");
+  int rc = ensure_eos(P->prm.nspec);
+  if (rc) return rc;
+  pcg::AuxArgs a{};
+  a.boxes = P->d_aux;
+  a.segs = P->d_aux_segs;
+  a.nseg = (int32_t)P->aux_segs.size();
+  a.partial = P->d_partial;
+  a.npartial = P->aux_blocks;
+  a.cfl = cfl;
+  a.dt_out = dt_dev;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = pcg_strict::launch_aux(AUX_ESTDT, P->prm.nspec, a, P->aux_blocks, s);
+  if (e == cudaSuccess) e = pcg_strict::launch_aux(AUX_ESTDT_FINAL, P->prm.nspec, a, 1, s);
+  return e == cudaSuccess ? PCG_OK : fail(PCG_ECUDA, "estdt: %s", cudaGetErrorString(e));
+}
+
+int pcg_plan_update(pcg_plan* P, const double* dt_dev, pcg_stream_t stream) {
+  if (!P) return fail(PCG_EINVAL, "plan is NULL");
+  int rc = ensure_eos(P->prm.nspec);
+  if (rc) return rc;
+  pcg::AuxArgs a{};
+  a.boxes = P->d_aux;
+  a.segs = P->d_aux_segs;
+  a.nseg = (int32_t)P->aux_segs.size();
+  a.dt_in = dt_dev;
+  cudaError_t e = pcg_strict::launch_aux(AUX_UPDATE, P->prm.nspec, a, P->aux_blocks, reinterpret_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? PCG_OK : fail(PCG_ECUDA, "update: %s", cudaGetErrorString(e));
+}
+
+int pcg_plan_info(const pcg_plan* P, int64_t* workspace_bytes, int32_t* nregions, int64_t* blocks_per_stage) {
+  if (!P) return fail(PCG_EINVAL, "plan is NULL");
+  if (workspace_bytes) *workspace_bytes = (int64_t)P->L.ws_bytes;
+  if (nregions) *nregions = (int32_t)P->L.regions.size();
+  if (blocks_per_stage)
+    for (int s = 0; s < K_NSTAGE; ++s) blocks_per_stage[s] = P->L.nblocks[s];
+  return PCG_OK;
+}
+
+int pcg_plan_destroy(pcg_plan* P) {
+  if (!P) return PCG_OK;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaSetDevice(P->device);
+  if (P->ws) cudaFree(P->ws);
+  if (P->T.dev) cudaFree(P->T.dev);
+  if (P->aux_dev) cudaFree(P->aux_dev);
+  cudaSetDevice(dev);
+  cudaGetLastError();
+  delete P;
+  return PCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,730 @@
+// pcg_kernels.cuh -- the stage kernels of the batched Godunov advance.
+//
+// One launch per stage covers every box of a batch: the launch's blocks are split
+// into segments (one region and one variant each, see pcg::Seg) so that uneven boxes
+// share a launch. Stages:
+//   K_CTOPRIM  pc_ctoprim on grow(box,4)                              -> q, qaux
+//   K_PREP     per cell of grow(box,1): shock flattening (3 directions) and the
+//              cell sound speed the trace uses; per node of the box: div u      -> prep, divu
+//   K_TRACE    trace_ppm / PLM, one direction per thread, grow(box,1)   -> trm[d], trp[d]
+//   K_FLUX0    first Riemann solve in each direction                    -> fi[d]
+//   K_FLUX1    pc_transdo + Riemann for both transverse partners of d  -> fdo[d][o]
+//   K_FLUX2    pc_transdd + final Riemann + pc_artif_visc + pc_norm_spec_flx
+//              + pc_ext_flx                                             -> ff[d], qec[d]
+//   K_CONSUP   pc_pdivu + pc_update                                     -> uout
+// Traced states are kept only for the cells whose states reach the box's fluxes
+// (grow(box,1)); the reference traces grow(box,2), whose outer layer feeds no output.
+// The per-cell quantities the reference recomputes in each of its three trace passes
+// (flatten, the cell sound speed) are computed once. EXACT selects the reference
+// expression order (parity form) or the reduced algebra (FMA / mixed forms).
+#pragma once
+
+#include "pcg_device.cuh"
+
+namespace PCG_TU {
+
+enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
+
+struct Item {
+  const pcg::Region* rg;
+  int variant;
+  int i, j, k;
+};
+
+// Timestep of a region and the constants the reference derives from it
+// (Source/Godunov.cpp:85-91, Source/PPM.cpp:37), with the same expressions.
+__device__ __forceinline__ double dt_of(const pcg::StageArgs& a, const pcg::Region& rg) {
+  return a.dt_dev ? *a.dt_dev : rg.dt;
+}
+
+__device__ __forceinline__ bool item_of(const pcg::StageArgs& a, Item& it) {
+  const int64_t blk = blockIdx.x;
+  int lo = 0, hi = a.nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.segs[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
+  }
+  const pcg::Seg& s = a.segs[lo];
+  const int64_t local = (blk - s.blk0) * blockDim.x + threadIdx.x;
+  if (local >= s.count) return false;
+  const int64_t t = local / s.n[0];
+  it.i = s.lo[0] + (int)(local - t * s.n[0]);
+  it.j = s.lo[1] + (int)(t % s.n[1]);
+  it.k = s.lo[2] + (int)(t / s.n[1]);
+  it.rg = a.regions + s.region;
+  it.variant = s.variant;
+  return true;
+}
+
+// A pointer positioned at one cell of a view: components n at p[n * ns].
+template <class T>
+struct CellPtr {
+  T* p;
+  int64_t ns;
+  __device__ __forceinline__ T& operator[](int n) const { return p[(int64_t)n * ns]; }
+};
+template <class T>
+__device__ __forceinline__ CellPtr<T> at(const V4<T>& v, int i, int j, int k) {
+  return CellPtr<T>{&v(i, j, k, 0), v.ns};
+}
+template <class T>
+__device__ __forceinline__ CellPtr<T> shift(const CellPtr<T>& c, int64_t off) {
+  return CellPtr<T>{c.p + off, c.ns};
+}
+template <class T>
+__device__ __forceinline__ int64_t dstride(const V4<T>& v, int d) {
+  return d == 0 ? 1 : d == 1 ? v.js : v.ks;
+}
+
+// ------------------------------------------------------------------ ctoprim
+// Source/PeleCUtilities.H:242-320 (pc_ctoprim), omega = rad = 0.
+template <int NS, bool MIX>
+__global__ void __launch_bounds__(128) k_ctoprim(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  const pcg::Region& rg = *it.rg;
+  using E = Eos<NS, MIX, double>;
+  const CellPtr<const double> u = at(v4<const double>(rg.uin), it.i, it.j, it.k);
+  const CellPtr<double> q = at(v4<double>(rg.q), it.i, it.j, it.k);
+  const CellPtr<double> qa = at(v4<double>(rg.qa), it.i, it.j, it.k);
+  const double rho = u[pcg::URHO];
+  const double rhoinv = 1.0 / rho;
+  const double vx = u[pcg::UMX] * rhoinv;
+  const double vy = u[pcg::UMY] * rhoinv;
+  const double vz = u[pcg::UMZ] * rhoinv;
+  const double kineng = 0.5 * rho * (vx * vx + vy * vy + vz * vz) - 0.5 * rho * 0.0 * 0.0 * 0.0 * 0.0;
+  q[pcg::QRHO] = rho;
+  q[pcg::QU] = vx;
+  q[pcg::QV] = vy;
+  q[pcg::QW] = vz;
+  double y[NS];
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    double yn = u[pcg::UFS + n] / rho;
+    if ((-1e-4 * DBL_EPSILON < yn) && (yn < 1e-4 * DBL_EPSILON)) yn = 0.0;
+    y[n] = yn;
+    q[pcg::QFS + n] = yn;
+  }
+  const double e = (u[pcg::UEDEN] - kineng) * rhoinv;
+  const double wbar = E::y2wbar(y);
+  const double T = E::rey2t(e, y, u[pcg::UTEMP]);
+  const double p = E::rty2p(rho, T, y);
+  const double cs = E::rty2cs(rho, T, y);
+  const double gam1 = E::rty2g(T, y);
+  double dpde, dpdr_e;
+  E::rty2dpde_dpdre(rho, T, y, dpde, dpdr_e);
+  q[pcg::QTEMP] = T;
+  q[pcg::QREINT] = e * rho;
+  q[pcg::QPRES] = p;
+  q[pcg::QGAME] = p / (e * rho) + 1.0;
+  qa[pcg::QDPDR] = dpdr_e;
+  qa[pcg::QDPDE] = dpde;
+  qa[pcg::QGAMC] = gam1;
+  qa[pcg::QC] = cs;
+  qa[pcg::QCSML] = dmax(pcg::SMALL_NUM, pcg::SMALL_NUM * cs);
+  qa[pcg::QRSPEC] = pcg::RU / wbar;
+}
+
+// ------------------------------------------------------------------ prep
+// Source/Hydro.H:476-517 (pc_divu) at node (i,j,k)
+__device__ __forceinline__ double divu_node(const V4<const double>& q, int i, int j, int k, const double* dx) {
+  const double ux = 0.25 *
+                    (q(i, j, k, pcg::QU) - q(i - 1, j, k, pcg::QU) + q(i, j, k - 1, pcg::QU) -
+                     q(i - 1, j, k - 1, pcg::QU) + q(i, j - 1, k, pcg::QU) - q(i - 1, j - 1, k, pcg::QU) +
+                     q(i, j - 1, k - 1, pcg::QU) - q(i - 1, j - 1, k - 1, pcg::QU)) /
+                    dx[0];
+  const double vy = 0.25 *
+                    (q(i, j, k, pcg::QV) - q(i, j - 1, k, pcg::QV) + q(i, j, k - 1, pcg::QV) -
+                     q(i, j - 1, k - 1, pcg::QV) + q(i - 1, j, k, pcg::QV) - q(i - 1, j - 1, k, pcg::QV) +
+                     q(i - 1, j, k - 1, pcg::QV) - q(i - 1, j - 1, k - 1, pcg::QV)) /
+                    dx[1];
+  const double wz = 0.25 *
+                    (q(i, j, k, pcg::QW) - q(i, j, k - 1, pcg::QW) + q(i - 1, j, k, pcg::QW) -
+                     q(i - 1, j, k - 1, pcg::QW) + q(i, j - 1, k, pcg::QW) - q(i, j - 1, k - 1, pcg::QW) +
+                     q(i - 1, j - 1, k, pcg::QW) - q(i - 1, j - 1, k - 1, pcg::QW)) /
+                    dx[2];
+  return ux + vy + wz;
+}
+
+// prep components: 0 = flattening (min over the 3 directions, Source/PPM.cpp:108-115),
+// 1 = sound speed the trace uses (PPM: RPY2Cs, Source/PPM.cpp:101; PLM: qaux QC).
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  const pcg::Region& rg = *it.rg;
+  const int i = it.i, j = it.j, k = it.k;
+  const V4<const double> q = v4<const double>(rg.q);
+  R flat = R(1);
+  if (a.use_flattening) {
+#pragma unroll
+    for (int df = 0; df < 3; df++) flat = dmin(flat, flatten<R>(q, i, j, k, df));
+  }
+  R cc;
+  if (a.ppm_type == 1) {
+    R y[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) y[n] = R(q(i, j, k, pcg::QFS + n));
+    const R rho = R(q(i, j, k, pcg::QRHO)), p = R(q(i, j, k, pcg::QPRES));
+    cc = EXACT ? Eos<NS, MIX, R>::rpy2cs(rho, p, y) : EosR<NS, MIX, R>::cs_y(rho, p, y);
+  } else {
+    cc = R(v4<const double>(rg.qa)(i, j, k, pcg::QC));
+  }
+  const CellPtr<R> pr = at(v4<R>(rg.prep), i, j, k);
+  pr[0] = flat;
+  pr[1] = cc;
+  if (i >= rg.lo[0] && i <= rg.hi[0] + 1 && j >= rg.lo[1] && j <= rg.hi[1] + 1 && k >= rg.lo[2] && k <= rg.hi[2] + 1)
+    v4<double>(rg.divu)(i, j, k) = divu_node(q, i, j, k, rg.dx);
+}
+
+// ------------------------------------------------------------------ trace
+template <class R>
+__device__ __forceinline__ void load5(const CellPtr<const double>& c, int64_t st, int n, R* s) {
+  const double* p = c.p + (int64_t)n * c.ns;
+#pragma unroll
+  for (int o = -2; o <= 2; ++o) s[o + 2] = R(p[o * st]);
+}
+
+// Source/PPM.cpp:82-423 for one cell and direction D (bx == vbx as called from
+// Source/Godunov.cpp:188-200, so both states are produced). Only the components the
+// path reads are reconstructed: QGAME, QREINT and QTEMP profiles feed nothing.
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, double dt) {
+  using E = Eos<NS, MIX, R>;
+  using ER = EosR<NS, MIX, R>;
+  const V4<const double> qv = v4<const double>(rg.q);
+  const CellPtr<const double> q = at(qv, i, j, k);
+  const int64_t st = dstride(qv, D);
+  const R dtdx = R(dt / rg.dx[D]);
+  const R un = R(q[pcg::QU + D]);
+  R s[5], sm, sp, s6;
+  R Imr[3], Ipr[3], Imu[3], Ipu[3], Imp[3], Ipp[3];
+  R Imt[3], Ipt[3];
+  const R sp3[3] = {un - cc, un, un + cc};
+#define PROFILE3(comp, Im, Ip)                                      \
+  load5<R>(q, st, comp, s);                                          \
+  ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);    \
+  s6 = ppm_s6<R>(sm, sp, s[2]);                                      \
+  _Pragma("unroll") for (int w = 0; w < 3; ++w) ppm_wave<R>(sm, sp, s6, sp3[w], dtdx, Ip[w], Im[w]);
+  PROFILE3(pcg::QRHO, Imr, Ipr)
+  PROFILE3(pcg::QU + D, Imu, Ipu)
+  PROFILE3(pcg::QPRES, Imp, Ipp)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (c == D) continue;
+    load5<R>(q, st, pcg::QU + c, s);
+    ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);
+    s6 = ppm_s6<R>(sm, sp, s[2]);
+    ppm_wave<R>(sm, sp, s6, un, dtdx, Ipt[c], Imt[c]);
+  }
+  R ym0[NS], ym1[NS], yp1[NS], yp2[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) {
+    R Im[3], Ip[3];
+    PROFILE3(pcg::QFS + n, Im, Ip)
+    ym0[n] = Im[0];
+    ym1[n] = Im[1];
+    yp1[n] = Ip[1];
+    yp2[n] = Ip[2];
+  }
+#undef PROFILE3
+  const CellPtr<R> qp = at(v4<R>(rg.trp[D]), i, j, k);
+  const CellPtr<R> qm = at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2));
+  // plus state on face i (Source/PPM.cpp:232-331)
+  {
+    R rho_ref = Imr[0];
+    const R un_ref = Imu[0];
+    R p_ref = Imp[0];
+    rho_ref = dmax(rho_ref, Lim<R>::tiny());
+    const R rho_ref_inv = R(1) / rho_ref;
+    p_ref = dmax(p_ref, Lim<R>::tiny());
+    const R cc_ref = EXACT ? E::rpy2cs(rho_ref, p_ref, ym0) : ER::cs_y(rho_ref, p_ref, ym0);
+    const R csq_ref = cc_ref * cc_ref;
+    const R cc_ref_inv = R(1) / cc_ref;
+    const R dum = un_ref - Imu[0];
+    const R dptotm = p_ref - Imp[0];
+    const R drho = rho_ref - Imr[1];
+    const R dptot = p_ref - Imp[1];
+    const R dup = un_ref - Imu[2];
+    const R dptotp = p_ref - Imp[2];
+    R alpham = R(0.5) * (dptotm * rho_ref_inv * cc_ref_inv - dum) * rho_ref * cc_ref_inv;
+    R alphap = R(0.5) * (dptotp * rho_ref_inv * cc_ref_inv + dup) * rho_ref * cc_ref_inv;
+    R alpha0r = drho - (EXACT ? dptot / csq_ref : dptot * cc_ref_inv * cc_ref_inv);
+    alpham = un - cc > R(0) ? R(0) : -alpham;
+    alphap = un + cc > R(0) ? R(0) : -alphap;
+    alpha0r = un > R(0) ? R(0) : -alpha0r;
+    const R rhos = dmax(Lim<R>::tiny(), rho_ref + alphap + alpham + alpha0r);
+    const R uns = un_ref + (alphap - alpham) * cc_ref * rho_ref_inv;
+    const R ps = dmax(Lim<R>::tiny(), p_ref + (alphap + alpham) * csq_ref);
+    qp[pcg::TR_RHO] = rhos;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) qp[pcg::TR_U + c] = (c == D) ? uns : Imt[c];
+    qp[pcg::TR_P] = ps;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) qp[pcg::TR_Y + n] = ym1[n];
+    qp[pcg::TR_RE] = EXACT ? rhos * E::ryp2e(rhos, ym1, ps) : ER::rhoe_y(rhos, ps, ym1);
+  }
+  // minus state on face i+1 (Source/PPM.cpp:334-422)
+  {
+    R rho_ref = Ipr[2];
+    const R un_ref = Ipu[2];
+    R p_ref = Ipp[2];
+    rho_ref = dmax(rho_ref, Lim<R>::tiny());
+    const R rho_ref_inv = R(1) / rho_ref;
+    p_ref = dmax(p_ref, Lim<R>::tiny());
+    const R cc_ref = EXACT ? E::rpy2cs(rho_ref, p_ref, yp2) : ER::cs_y(rho_ref, p_ref, yp2);
+    const R csq_ref = cc_ref * cc_ref;
+    const R cc_ref_inv = R(1) / cc_ref;
+    const R dum = un_ref - Ipu[0];
+    const R dptotm = p_ref - Ipp[0];
+    const R drho = rho_ref - Ipr[1];
+    const R dptot = p_ref - Ipp[1];
+    const R dup = un_ref - Ipu[2];
+    const R dptotp = p_ref - Ipp[2];
+    R alpham = R(0.5) * (dptotm * rho_ref_inv * cc_ref_inv - dum) * rho_ref * cc_ref_inv;
+    R alphap = R(0.5) * (dptotp * rho_ref_inv * cc_ref_inv + dup) * rho_ref * cc_ref_inv;
+    R alpha0r = drho - (EXACT ? dptot / csq_ref : dptot * cc_ref_inv * cc_ref_inv);
+    alpham = un - cc > R(0) ? -alpham : R(0);
+    alphap = un + cc > R(0) ? -alphap : R(0);
+    alpha0r = un > R(0) ? -alpha0r : R(0);
+    const R rhos = dmax(Lim<R>::tiny(), rho_ref + alphap + alpham + alpha0r);
+    const R uns = un_ref + (alphap - alpham) * cc_ref * rho_ref_inv;
+    const R ps = dmax(Lim<R>::tiny(), p_ref + (alphap + alpham) * csq_ref);
+    qm[pcg::TR_RHO] = rhos;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) qm[pcg::TR_U + c] = (c == D) ? uns : Ipt[c];
+    qm[pcg::TR_P] = ps;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) qm[pcg::TR_Y + n] = yp1[n];
+    qm[pcg::TR_RE] = EXACT ? rhos * E::ryp2e(rhos, yp1, ps) : ER::rhoe_y(rhos, ps, yp1);
+  }
+}
+
+// Source/PLM.H:167-309 (pc_plm_d) with the slopes of Source/Godunov.cpp:139-180.
+template <int NS, int D, class R>
+__device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
+                                              double dt) {
+  constexpr int l1 = (D == 0) ? 1 : 0;
+  constexpr int l2 = (D == 2) ? 1 : 2;
+  const V4<const double> qv = v4<const double>(rg.q);
+  const CellPtr<const double> q = at(qv, i, j, k);
+  const int64_t st = dstride(qv, D);
+  R s[5];
+#define SLOPE(comp) (load5<R>(q, st, comp, s), plm_slope<R>(s[0], s[1], s[2], s[3], s[4], flat, order))
+  const R drho = SLOPE(pcg::QRHO);
+  const R dvel[3] = {SLOPE(pcg::QU), SLOPE(pcg::QV), SLOPE(pcg::QW)};
+  const R dp = SLOPE(pcg::QPRES);
+  const R drhoe = SLOPE(pcg::QREINT);
+  const R dtdx = R(dt / rg.dx[D]);
+  const R cs = cc * cc;
+  const R rho = R(q[pcg::QRHO]);
+  const R vel[3] = {R(q[pcg::QU]), R(q[pcg::QV]), R(q[pcg::QW])};
+  const R p = R(q[pcg::QPRES]);
+  const R rhoe = R(q[pcg::QREINT]);
+  const R enth = ((rhoe + p) / rho) / cs;
+  const R alpham = R(0.5) * (dp / (rho * cc) - dvel[D]) * rho / cc;
+  const R alphap = R(0.5) * (dp / (rho * cc) + dvel[D]) * rho / cc;
+  const R alpha0r = drho - dp / cs;
+  const R alpha0e = drhoe - dp * enth;
+  const R alpha0v = dvel[l1];
+  const R alpha0w = dvel[l2];
+  const R wv[3] = {vel[D] - cc, vel[D], vel[D] + cc};
+  const CellPtr<R> qp = at(v4<R>(rg.trp[D]), i, j, k);
+  const CellPtr<R> qm = at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2));
+  {
+    const R rho_ref = rho - R(0.5) * (R(1) + dtdx * dmin(wv[0], R(0))) * drho;
+    R vel_ref[3];
+#pragma unroll
+    for (int dim = 0; dim < 3; dim++) vel_ref[dim] = vel[dim] - R(0.5) * (R(1) + dtdx * dmin(wv[0], R(0))) * dvel[dim];
+    const R p_ref = p - R(0.5) * (R(1) + dtdx * dmin(wv[0], R(0))) * dp;
+    const R rhoe_ref = rhoe - R(0.5) * (R(1) + dtdx * dmin(wv[0], R(0))) * drhoe;
+    const R apright = R(0.25) * dtdx * (wv[0] - wv[2]) * (R(1) - copysign(R(1), wv[2])) * alphap;
+    const R amright = R(0);
+    const R azrright = R(0.25) * dtdx * (wv[0] - wv[1]) * (R(1) - copysign(R(1), wv[1])) * alpha0r;
+    const R azeright = R(0.25) * dtdx * (wv[0] - wv[1]) * (R(1) - copysign(R(1), wv[1])) * alpha0e;
+    const R azv1rght = R(0.25) * dtdx * (wv[0] - wv[1]) * (R(1) - copysign(R(1), wv[1])) * alpha0v;
+    const R azw1rght = R(0.25) * dtdx * (wv[0] - wv[1]) * (R(1) - copysign(R(1), wv[1])) * alpha0w;
+    R r = rho_ref + apright + amright + azrright;
+    qp[pcg::TR_RHO] = dmax(Lim<R>::tiny(), r);
+    qp[pcg::TR_U + D] = vel_ref[D] + (apright - amright) * cc / rho;
+    qp[pcg::TR_U + l1] = vel_ref[l1] + azv1rght;
+    qp[pcg::TR_U + l2] = vel_ref[l2] + azw1rght;
+    r = p_ref + (apright + amright) * cs;
+    qp[pcg::TR_P] = dmax(r, Lim<R>::tiny());
+    qp[pcg::TR_RE] = rhoe_ref + (apright + amright) * enth * cs + azeright;
+  }
+  {
+    const R rho_ref = rho + R(0.5) * (R(1) - dtdx * dmax(wv[2], R(0))) * drho;
+    R vel_ref[3];
+#pragma unroll
+    for (int dim = 0; dim < 3; dim++) vel_ref[dim] = vel[dim] + R(0.5) * (R(1) - dtdx * dmax(wv[2], R(0))) * dvel[dim];
+    const R p_ref = p + R(0.5) * (R(1) - dtdx * dmax(wv[2], R(0))) * dp;
+    const R rhoe_ref = rhoe + R(0.5) * (R(1) - dtdx * dmax(wv[2], R(0))) * drhoe;
+    const R apleft = R(0);
+    const R amleft = R(0.25) * dtdx * (wv[2] - wv[0]) * (R(1) + copysign(R(1), wv[0])) * alpham;
+    const R azrleft = R(0.25) * dtdx * (wv[2] - wv[1]) * (R(1) + copysign(R(1), wv[1])) * alpha0r;
+    const R azeleft = R(0.25) * dtdx * (wv[2] - wv[1]) * (R(1) + copysign(R(1), wv[1])) * alpha0e;
+    const R azv1left = R(0.25) * dtdx * (wv[2] - wv[1]) * (R(1) + copysign(R(1), wv[1])) * alpha0v;
+    const R azw1left = R(0.25) * dtdx * (wv[2] - wv[1]) * (R(1) + copysign(R(1), wv[1])) * alpha0w;
+    R r = rho_ref + apleft + amleft + azrleft;
+    qm[pcg::TR_RHO] = dmax(r, Lim<R>::tiny());
+    qm[pcg::TR_U + D] = vel_ref[D] + (apleft - amleft) * cc / rho;
+    qm[pcg::TR_U + l1] = vel_ref[l1] + azv1left;
+    qm[pcg::TR_U + l2] = vel_ref[l2] + azw1left;
+    r = p_ref + (apleft + amleft) * cs;
+    qm[pcg::TR_P] = dmax(r, Lim<R>::tiny());
+    qm[pcg::TR_RE] = rhoe_ref + (apleft + amleft) * enth * cs + azeleft;
+  }
+  const R vel_ad = R(q[pcg::QU + D]);
+  const R spzerom = (vel_ad > R(0)) ? R(-1) : vel_ad * dtdx;
+  const R spzerop = (vel_ad >= R(0)) ? vel_ad * dtdx : R(1);
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    const R slope = SLOPE(pcg::QFS + n);
+    const R qc = R(q[pcg::QFS + n]);
+    const R acmprght = R(0.5) * (R(-1) - spzerom) * slope;
+    qp[pcg::TR_Y + n] = qc + acmprght;
+    const R acmpleft = R(0.5) * (R(1) - spzerop) * slope;
+    qm[pcg::TR_Y + n] = qc + acmpleft;
+  }
+#undef SLOPE
+}
+
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void trace_cell(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+  const CellPtr<const R> pr = at(v4<const R>(rg.prep), i, j, k);
+  const R flat = pr[0], cc = pr[1];
+  const double dt = dt_of(a, rg);
+  if (a.ppm_type == 1)
+    trace_ppm_dir<NS, MIX, EXACT, D, R>(rg, i, j, k, cc, flat, dt);
+  else
+    trace_plm_dir<NS, D, R>(rg, i, j, k, cc, flat, a.plm_iorder, dt);
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_trace(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  switch (it.variant) {
+    case 0: trace_cell<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: trace_cell<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+    default: trace_cell<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  }
+}
+
+// ------------------------------------------------------------------ flux stages
+template <int NS, class R>
+__device__ __forceinline__ void load_state(const CellPtr<R>& t, R* s) {
+#pragma unroll
+  for (int n = 0; n < pcg::nt_comps(NS); ++n) s[n] = t[n];
+}
+
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void face_flux(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr,
+                                          R* fl, R& gun, R& gpres) {
+  const V4<const double> qav = v4<const double>(rg.qa);
+  const CellPtr<const double> qa = at(qav, i, j, k);
+  const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + (int64_t)pcg::QC * qa.ns]));
+  const int idx = (D == 0) ? i : (D == 1) ? j : k;
+  cmpflx<NS, MIX, EXACT, D, R>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav, fl, gun, gpres);
+}
+
+template <int NS, class R>
+__device__ __forceinline__ void store_tflux(const CellPtr<R>& f, const R* fl, R gun, R gpres) {
+#pragma unroll
+  for (int n = 0; n < 5; ++n) f[n] = fl[n];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) f[pcg::FL_Y + n] = fl[pcg::UFS + n];
+  f[pcg::FL_Y + NS] = gpres;
+  f[pcg::FL_Y + NS + 1] = gun;
+}
+
+// First Riemann solves (Source/Godunov.cpp:206-244).
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void flux0_face(const pcg::Region& rg, int i, int j, int k) {
+  R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)], fl[pcg::nvar(NS)], gun, gpres;
+  load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), ql);
+  load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qr);
+  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, fl, gun, gpres);
+  store_tflux<NS, R>(at(v4<R>(rg.fi[D]), i, j, k), fl, gun, gpres);
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_flux0(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  switch (it.variant) {
+    case 0: flux0_face<NS, MIX, EXACT, 0, R>(*it.rg, it.i, it.j, it.k); break;
+    case 1: flux0_face<NS, MIX, EXACT, 1, R>(*it.rg, it.i, it.j, it.k); break;
+    default: flux0_face<NS, MIX, EXACT, 2, R>(*it.rg, it.i, it.j, it.k); break;
+  }
+}
+
+// Source/Godunov.H:455-633 (pc_transdo) for one side: qn is the traced state, f the
+// O-flux positioned at the cell's low O-face (its high O-face is at +ostride).
+template <int NS, bool EXACT, class R>
+__device__ __forceinline__ void transdo_side(const R* qn, const CellPtr<const R>& f, int64_t ostride, R cdtdx, R c,
+                                             R* out) {
+  const CellPtr<const R> g = shift(f, ostride);
+  const R flxrho = cdtdx * (g[0] - f[0]);
+  const R flxu = cdtdx * (g[1] - f[1]);
+  const R flxv = cdtdx * (g[2] - f[2]);
+  const R flxw = cdtdx * (g[3] - f[3]);
+  const R flxe = cdtdx * (g[4] - f[4]);
+  const R rr = qn[pcg::TR_RHO];
+  const R rrnew = rr - flxrho;
+  const R irrnew = EXACT ? R(0) : rrcp(rrnew);
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    const R compn = cdtdx * (g[pcg::FL_Y + n] - f[pcg::FL_Y + n]);
+    const R compo = rr * qn[pcg::TR_Y + n] - compn;
+    out[pcg::TR_Y + n] = EXACT ? compo / rrnew : compo * irrnew;
+  }
+  const R pggp = g[pcg::FL_Y + NS];
+  const R pggm = f[pcg::FL_Y + NS];
+  const R ugp = g[pcg::FL_Y + NS + 1];
+  const R ugm = f[pcg::FL_Y + NS + 1];
+  const R dAup = pggp * ugp - pggm * ugm;
+  const R pav = R(0.5) * (pggp + pggm);
+  const R dAu = ugp - ugm;
+  R ru = qn[pcg::TR_U], rv = qn[pcg::TR_V], rw = qn[pcg::TR_W];
+  const R ekin = R(0.5) * rr * (ru * ru + rv * rv + rw * rw);
+  ru *= rr;
+  rv *= rr;
+  rw *= rr;
+  const R re = qn[pcg::TR_RE] + ekin;
+  const R runew = ru - flxu;
+  const R rvnew = rv - flxv;
+  const R rwnew = rw - flxw;
+  const R renew = re - flxe;
+  out[pcg::TR_RHO] = rrnew;
+  out[pcg::TR_U] = EXACT ? runew / rrnew : runew * irrnew;
+  out[pcg::TR_V] = EXACT ? rvnew / rrnew : rvnew * irrnew;
+  out[pcg::TR_W] = EXACT ? rwnew / rrnew : rwnew * irrnew;
+  const R ke2 = runew * runew + rvnew * rvnew + rwnew * rwnew;
+  const R rhoekin = EXACT ? R(0.5) * ke2 / rrnew : R(0.5) * ke2 * irrnew;
+  out[pcg::TR_RE] = renew - rhoekin;
+  const R pnew = qn[pcg::TR_P] - cdtdx * (dAup + pav * dAu * (c - R(1)));
+  out[pcg::TR_P] = dmax(pnew, Lim<R>::very_small());
+}
+
+// Transverse predictor + paired Riemann solve for the pair (D|O) at D-face (i,j,k)
+// (Source/Godunov.cpp:246-384).
+template <int NS, bool MIX, bool EXACT, int D, int O, class R>
+__device__ __forceinline__ void flux1_pair(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+  const V4<const double> qav = v4<const double>(rg.qa);
+  const V4<const R> fov = v4<const R>(rg.fi[O]);
+  const int64_t dst_f = dstride(fov, D), ost_f = dstride(fov, O);
+  const CellPtr<const R> fo = at(fov, i, j, k);
+  const CellPtr<const double> qa = at(qav, i, j, k);
+  const R cdt = R(1.0 / 3.0 * dt_of(a, rg) / rg.dx[O]);
+  R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+  load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
+  transdo_side<NS, EXACT, R>(qn, shift(fo, -dst_f), ost_f, cdt,
+                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), ql);
+  load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qn);
+  transdo_side<NS, EXACT, R>(qn, fo, ost_f, cdt, R(qa[pcg::QGAMC]), qr);
+  R fl[pcg::nvar(NS)], gun, gpres;
+  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, fl, gun, gpres);
+  store_tflux<NS, R>(at(v4<R>(rg.fdo[D][O]), i, j, k), fl, gun, gpres);
+}
+
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void flux1_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+  constexpr int O1 = (D == 0) ? 1 : 0;
+  constexpr int O2 = (D == 2) ? 1 : 2;
+  const int c[3] = {i, j, k};
+  // fdo[D][O] covers O in the box and the third direction grown by one
+  if (c[O1] >= rg.lo[O1] && c[O1] <= rg.hi[O1]) flux1_pair<NS, MIX, EXACT, D, O1, R>(a, rg, i, j, k);
+  if (c[O2] >= rg.lo[O2] && c[O2] <= rg.hi[O2]) flux1_pair<NS, MIX, EXACT, D, O2, R>(a, rg, i, j, k);
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_flux1(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  switch (it.variant) {
+    case 0: flux1_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: flux1_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+    default: flux1_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  }
+}
+
+// Source/Godunov.H:639-845 (pc_transdd) for one side: fx is the O1-flux corrected by
+// O2 positioned at the cell's low O1-face, fy the O2-flux corrected by O1 at the low
+// O2-face.
+template <int NS, bool EXACT, class R>
+__device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>& fx, int64_t xst,
+                                             const CellPtr<const R>& fy, int64_t yst, R cdtdx0, R cdtdx1, R hdt,
+                                             R c, bool has_src, const CellPtr<const double>& sq, R* out) {
+  const CellPtr<const R> gx = shift(fx, xst), gy = shift(fy, yst);
+#define FD(n) (cdtdx0 * (gx[n] - fx[n]) + cdtdx1 * (gy[n] - fy[n]))
+  const R flxrho = FD(0);
+  const R flxu = FD(1);
+  const R flxv = FD(2);
+  const R flxw = FD(3);
+  const R flxe = FD(4);
+  const R rr = qn[pcg::TR_RHO];
+  const R rrnew = rr - flxrho;
+  const R irrnew = EXACT ? R(0) : rrcp(rrnew);
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    const R srcpass = has_src ? R(sq[pcg::QFS + n]) : R(0);
+    const R compn = FD(pcg::FL_Y + n);
+    const R compo = rr * qn[pcg::TR_Y + n] - compn;
+    out[pcg::TR_Y + n] = (EXACT ? compo / rrnew : compo * irrnew) + hdt * srcpass;
+  }
+#undef FD
+  const int gp = pcg::FL_Y + NS, gu = pcg::FL_Y + NS + 1;
+  const R dAupx = gx[gp] * gx[gu] - fx[gp] * fx[gu];
+  const R pavx = R(0.5) * (gx[gp] + fx[gp]);
+  const R dAux = gx[gu] - fx[gu];
+  const R dAupy = gy[gp] * gy[gu] - fy[gp] * fy[gu];
+  const R pavy = R(0.5) * (gy[gp] + fy[gp]);
+  const R dAuy = gy[gu] - fy[gu];
+  const R pxnew = cdtdx0 * (dAupx + pavx * dAux * (c - R(1)));
+  const R pynew = cdtdx1 * (dAupy + pavy * dAuy * (c - R(1)));
+  const R s0 = has_src ? R(sq[pcg::QRHO]) : R(0), s1 = has_src ? R(sq[pcg::QU]) : R(0);
+  const R s2 = has_src ? R(sq[pcg::QV]) : R(0), s3 = has_src ? R(sq[pcg::QW]) : R(0);
+  const R s4 = has_src ? R(sq[pcg::QREINT]) : R(0), s5 = has_src ? R(sq[pcg::QPRES]) : R(0);
+  const R ru = rr * qn[pcg::TR_U];
+  const R rv = rr * qn[pcg::TR_V];
+  const R rw = rr * qn[pcg::TR_W];
+  const R ekin2 = ru * ru + rv * rv + rw * rw;
+  const R ekin = EXACT ? R(0.5) * ekin2 / rr : R(0.5) * ekin2 * rrcp(rr);
+  const R re = qn[pcg::TR_RE] + ekin;
+  const R runew = ru - flxu;
+  const R rvnew = rv - flxv;
+  const R rwnew = rw - flxw;
+  const R renew = re - flxe;
+  out[pcg::TR_RHO] = rrnew + hdt * s0;
+  out[pcg::TR_U] = (EXACT ? runew / rrnew : runew * irrnew) + hdt * s1;
+  out[pcg::TR_V] = (EXACT ? rvnew / rrnew : rvnew * irrnew) + hdt * s2;
+  out[pcg::TR_W] = (EXACT ? rwnew / rrnew : rwnew * irrnew) + hdt * s3;
+  const R ke2 = runew * runew + rvnew * rvnew + rwnew * rwnew;
+  const R rhoekin = EXACT ? R(0.5) * ke2 / rrnew : R(0.5) * ke2 * irrnew;
+  out[pcg::TR_RE] = renew - rhoekin + hdt * s4;
+  const R pn = qn[pcg::TR_P] - pxnew - pynew + hdt * s5;
+  out[pcg::TR_P] = dmax(pn, Lim<R>::tiny());
+}
+
+// Final fluxes (Source/Godunov.cpp:392-438) followed by the per-face flux adjustments
+// of pc_adjust_fluxes (Source/Hydro.cpp:380-413): pc_artif_visc (Godunov.H:1067-1138),
+// pc_norm_spec_flx and pc_ext_flx (Hydro.H:835-865), all in FP64.
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+  constexpr int O1 = (D == 0) ? 1 : 0;
+  constexpr int O2 = (D == 2) ? 1 : 2;
+  const V4<const double> qav = v4<const double>(rg.qa);
+  const CellPtr<const double> qa = at(qav, i, j, k);
+  const V4<const R> fxv = v4<const R>(rg.fdo[O1][O2]);
+  const V4<const R> fyv = v4<const R>(rg.fdo[O2][O1]);
+  const CellPtr<const R> fx = at(fxv, i, j, k), fy = at(fyv, i, j, k);
+  const int64_t xd = dstride(fxv, D), yd = dstride(fyv, D);
+  const int64_t xst = dstride(fxv, O1), yst = dstride(fyv, O2);
+  const double dt = dt_of(a, rg);
+  const R cdtdx0 = R(0.5 * dt / rg.dx[O1]);
+  const R cdtdx1 = R(0.5 * dt / rg.dx[O2]);
+  const R hdt = R(0.5 * dt);
+  const bool has_src = rg.srcq.p != nullptr;
+  const V4<const double> sqv = v4<const double>(rg.srcq);
+  const CellPtr<const double> sqp = has_src ? at(sqv, i, j, k) : CellPtr<const double>{nullptr, 0};
+  const CellPtr<const double> sqm = has_src ? shift(sqp, -dstride(sqv, D)) : sqp;
+  R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+  load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
+  transdd_side<NS, EXACT, R>(qn, shift(fx, -xd), xst, shift(fy, -yd), yst, cdtdx0, cdtdx1, hdt,
+                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), has_src, sqm, ql);
+  load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qn);
+  transdd_side<NS, EXACT, R>(qn, fx, xst, fy, yst, cdtdx0, cdtdx1, hdt, R(qa[pcg::QGAMC]), has_src, sqp, qr);
+  R flr[pcg::nvar(NS)], gun, gpres;
+  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, flr, gun, gpres);
+  double fl[pcg::nvar(NS)];
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) fl[n] = (n == pcg::UTEMP) ? 0.0 : double(flr[n]);
+  // pc_artif_visc
+  const V4<const double> dv = v4<const double>(rg.divu);
+  const int ji = i + (O1 == 0), jj = j + (O1 == 1), jk = k + (O1 == 2);
+  const int ki = i + (O2 == 0), kj = j + (O2 == 1), kk = k + (O2 == 2);
+  const double div =
+    a.difmag * dmin(0.0, 0.25 * (dv(i, j, k) + dv(ji, jj, jk) + dv(ki, kj, kk) +
+                                 dv(ji + (O2 == 0), jj + (O2 == 1), jk + (O2 == 2))));
+  const int idx = (D == 0) ? i : (D == 1) ? j : k;
+  const bool at_bndry = (idx == rg.domlo[D] && rg.bclo[D] == pcg::BC_NO_SLIP_WALL) ||
+                        (idx == rg.domhi[D] + 1 && rg.bchi[D] == pcg::BC_NO_SLIP_WALL);
+  const double dxd = rg.dx[D];
+  const V4<const double> uv = v4<const double>(rg.uin);
+  const CellPtr<const double> u = at(uv, i, j, k);
+  const int64_t ud = dstride(uv, D);
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); n++) {
+    if (n == pcg::UTEMP) continue;
+    const bool is_tang = (n == pcg::UMX || n == pcg::UMY || n == pcg::UMZ) && (n != pcg::UMX + D);
+    if (!(at_bndry && is_tang)) fl[n] += dxd * div * (u[n] - u.p[-ud + (int64_t)n * u.ns]);
+  }
+  fl[pcg::UTEMP] = 0.0;
+  // pc_norm_spec_flx
+  double summ = 0.0;
+#pragma unroll
+  for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) summ += fl[n];
+  const double fac = (summ != 0.0) ? fl[pcg::URHO] / summ : 1.0;
+#pragma unroll
+  for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) fl[n] *= fac;
+  // pc_ext_flx
+  const double ar = rg.area[D].p ? v4<const double>(rg.area[D])(i, j, k) : rg.area_u[D];
+  const CellPtr<double> ff = at(v4<double>(rg.ff[D]), i, j, k);
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = fl[n] * ar;
+  const CellPtr<double> qe = at(v4<double>(rg.qec[D]), i, j, k);
+  qe[0] = double(gpres);
+  qe[1] = double(gun);
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_flux2(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  switch (it.variant) {
+    case 0: flux2_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: flux2_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+    default: flux2_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  }
+}
+
+// Source/Godunov.H:1033-1060 (pc_pdivu) and Source/Hydro.H:888-907 (pc_update).
+template <int NS>
+__global__ void __launch_bounds__(128) k_consup(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  const pcg::Region& rg = *it.rg;
+  const int i = it.i, j = it.j, k = it.k;
+  const V4<const double> f0v = v4<const double>(rg.ff[0]), f1v = v4<const double>(rg.ff[1]),
+                         f2v = v4<const double>(rg.ff[2]);
+  const CellPtr<const double> f0 = at(f0v, i, j, k), f1 = at(f1v, i, j, k), f2 = at(f2v, i, j, k);
+  const CellPtr<const double> f0p = shift(f0, 1), f1p = shift(f1, f1v.js), f2p = shift(f2, f2v.ks);
+  const V4<const double> q0v = v4<const double>(rg.qec[0]), q1v = v4<const double>(rg.qec[1]),
+                         q2v = v4<const double>(rg.qec[2]);
+  const CellPtr<const double> q0 = at(q0v, i, j, k), q1 = at(q1v, i, j, k), q2 = at(q2v, i, j, k);
+  const CellPtr<const double> q0p = shift(q0, 1), q1p = shift(q1, q1v.js), q2p = shift(q2, q2v.ks);
+  const bool ua = rg.area[0].p != nullptr;
+  const V4<const double> a0 = v4<const double>(rg.area[0]);
+  const V4<const double> a1 = v4<const double>(rg.area[1]);
+  const V4<const double> a2 = v4<const double>(rg.area[2]);
+  const double a0m = ua ? a0(i, j, k) : rg.area_u[0], a0p = ua ? a0(i + 1, j, k) : rg.area_u[0];
+  const double a1m = ua ? a1(i, j, k) : rg.area_u[1], a1p = ua ? a1(i, j + 1, k) : rg.area_u[1];
+  const double a2m = ua ? a2(i, j, k) : rg.area_u[2], a2p = ua ? a2(i, j, k + 1) : rg.area_u[2];
+  const double v = rg.vol.p ? v4<const double>(rg.vol)(i, j, k) : rg.vol_u;
+  const double pdivu = 0.5 *
+                       ((q0p[0] + q0[0]) * (q0p[1] * a0p - q0[1] * a0m) +
+                        (q1p[0] + q1[0]) * (q1p[1] * a1p - q1[1] * a1m) +
+                        (q2p[0] + q2[0]) * (q2p[1] * a2p - q2[1] * a2m)) /
+                       v;
+  const CellPtr<double> uo = at(v4<double>(rg.uout), i, j, k);
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) {
+    const double old = rg.zero_uout ? 0.0 : uo[n];
+    uo[n] = old + (f0[n] - f0p[n] + f1[n] - f1p[n] + f2[n] - f2p[n]) / v;
+  }
+  uo[pcg::UEINT] -= pdivu;
+}
+
+}  // namespace PCG_TU

@@ -1,0 +1,143 @@
+// pcg_types.h -- layouts shared by the host runtime and the device kernels.
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define PCG_HD __host__ __device__
+#else
+#define PCG_HD
+#endif
+
+namespace pcg {
+
+// Source/IndexDefines.H:6-89 (NUM_ADV = NUM_AUX = NUM_LIN = 0)
+enum { URHO = 0, UMX = 1, UMY = 2, UMZ = 3, UEDEN = 4, UEINT = 5, UTEMP = 6, UFS = 7 };
+enum { QRHO = 0, QU = 1, QV = 2, QW = 3, QGAME = 4, QPRES = 5, QREINT = 6, QTEMP = 7, QFS = 8 };
+enum { QGAMC = 0, QC = 1, QCSML = 2, QDPDR = 3, QDPDE = 4, QRSPEC = 5, NQAUX = 6 };
+// Source/PeleC.H:49-57
+enum { BC_INTERIOR = 0, BC_INFLOW, BC_OUTFLOW, BC_SYMMETRY, BC_SLIP_WALL, BC_NO_SLIP_WALL, BC_USER };
+
+// Face-state layout of the traced states (qm/qp of the reference, only the components
+// the path reads): rho, u, v, w, p, rho*e, Y[NS].
+enum { TR_RHO = 0, TR_U = 1, TR_V = 2, TR_W = 3, TR_P = 4, TR_RE = 5, TR_Y = 6 };
+// Transverse-flux layout: URHO, UMX, UMY, UMZ, UEDEN (same indices as U), then Y[NS]
+// at FL_Y, then the Godunov pressure and normal velocity (qint GDPRES / GDU..GDW).
+enum { FL_Y = 5 };
+PCG_HD constexpr int nt_comps(int ns) { return 6 + ns; }
+PCG_HD constexpr int nf_comps(int ns) { return 7 + ns; }
+PCG_HD constexpr int nvar(int ns) { return 7 + ns; }
+PCG_HD constexpr int qvar(int ns) { return 8 + ns; }
+
+// Source/Constants.H:18-30
+constexpr double SMALLU = 1.0e-12;
+constexpr double SMALL_NUM = 1.0e-8;
+constexpr double VERY_SMALL_NUM = 2.220446049250313080847263336181640625e-16 * 1e-100;
+
+// EOS restatement constants (same as the oracle)
+constexpr double RU = 8.31446261815324e7;
+constexpr int NEWTON_MAXIT = 20;
+constexpr double NEWTON_RTOL = 1.0e-10;
+constexpr double NEWTON_TMIN = 10.0;
+constexpr int MAXNS = 16;
+
+struct EosConst {
+  int kind;  // 0 gamma law, 1 NASA-7 mixture
+  int nspec;
+  double gamma;
+  double imw[MAXNS];
+  double tmid[MAXNS];
+  double cvc[MAXNS][2][5];
+  double ec[MAXNS][2][6];
+  float gammaf;
+  float imwf[MAXNS];
+  float tmidf[MAXNS];
+  float cvcf[MAXNS][2][5];
+  float ecf[MAXNS][2][6];
+};
+
+// A strided block of memory addressed like amrex::Array4 (element type decided by the
+// kernel that reads it): p[(i-b0) + (j-b1)*js + (k-b2)*ks + n*ns].
+struct View {
+  void* p;
+  int64_t js, ks, ns;
+  int32_t b[3];
+  int32_t pad;
+};
+
+// Everything one box of a launch needs. Workspace views point into the library's
+// workspace; in/out views may be the caller's arrays.
+struct Region {
+  int32_t lo[3], hi[3];
+  int32_t domlo[3], domhi[3], bclo[3], bchi[3];
+  double dx[3];
+  double dt;        // used unless StageArgs::dt_dev is set
+  double area_u[3]; // uniform face areas (used when area[d].p == nullptr)
+  double vol_u;     // uniform volume (used when vol.p == nullptr)
+  View uin;         // conserved state, double, >= 4 ghosts
+  View uout;        // hydro source, double, valid box
+  View q;           // primitive state, double, QVAR comps on >= grow(box,4)
+  View qa;          // auxiliary state, double, NQAUX comps
+  View srcq;        // primitive sources (p == nullptr: none)
+  View prep;        // flattening and trace sound speed on grow(box,1), compute type
+  View divu;        // nodal div u on the box's nodes, double
+  View area[3];     // face areas (p == nullptr: uniform)
+  View vol;         // cell volumes (p == nullptr: uniform)
+  View trm[3];      // traced minus (left) states on the d-faces, compute type
+  View trp[3];      // traced plus (right) states on the d-faces, compute type
+  View fi[3];       // initial d-fluxes, compute type
+  View fdo[3][3];   // d-fluxes from d-states corrected by o-fluxes, compute type
+  View ff[3];       // final fluxes, double, NVAR comps (area-weighted)
+  View qec[3];      // Godunov pressure and normal velocity at final faces, double
+  int32_t zero_uout; // 1: write uout (=), 0: accumulate (+=)
+  int32_t pad;
+};
+
+// A run of thread blocks of one stage working on one region (and one variant, e.g.
+// a direction or a (direction, other direction) pair) over the index box
+// [lo, lo + n).
+struct Seg {
+  int32_t region;
+  int32_t variant;
+  int32_t lo[3];
+  int32_t n[3];
+  int64_t count;
+  int64_t blk0;  // first block of this segment within the launch
+};
+
+struct StageArgs {
+  const Region* regions;
+  const Seg* segs;
+  int32_t nseg;
+  int32_t ppm_type;
+  int32_t plm_iorder;
+  int32_t use_flattening;
+  double difmag;
+  const double* dt_dev;  // nullptr: each region's dt
+};
+
+// One box for the auxiliary kernels (timestep, state update).
+struct AuxBox {
+  int32_t lo[3], hi[3];
+  double dx[3];
+  double dt;
+  View uin;   // S_old
+  View uout;  // hydro source
+  View snew;  // S_new (may alias uin)
+};
+
+struct AuxArgs {
+  const AuxBox* boxes;
+  const Seg* segs;
+  int32_t nseg;
+  int32_t dir;          // ghost fill: direction
+  double* partial;      // timestep: one minimum per block
+  int64_t npartial;
+  double cfl;
+  double* dt_out;       // timestep result (device)
+  const double* dt_in;  // state update: device dt (nullptr: per-box dt)
+  View state;           // ghost fill: domain FAB
+  int32_t dlo[3], dhi[3], ng, periodic, ncomp;
+};
+
+}  // namespace pcg

@@ -218,6 +218,7 @@ class Patch:
     lo: tuple
     hi: tuple
     fab: abi.Fab  # conserved state on grow([lo,hi], NG)
+    dx: tuple = (FLAME_DX,) * 3
 
     @property
     def ncells(self):
@@ -289,3 +290,42 @@ def turbulence(n=256, box=64, seed=4, kmax=32, mach=0.3, gamma=1.4) -> Level:
                 state, tile_boxes((n, n, n), (box, box, box)), (True, True, True))
     lev.fill_ghosts()
     return lev
+
+
+# ------------------------------------------------------------------ generic random states (tests)
+def _smooth_noise(rng, shape, passes=2):
+    a = rng.standard_normal(shape)
+    for _ in range(passes):
+        for ax in range(3):
+            a = 0.25 * np.roll(a, 1, axis=ax) + 0.5 * a + 0.25 * np.roll(a, -1, axis=ax)
+    return a / (np.abs(a).max() + 1e-300)
+
+
+def random_patch(edges, seed, eos=None, shock=True) -> Patch:
+    """A box with smooth random primitive fields plus (optionally) a pressure jump, so
+    every limiter, flattening and Riemann branch is exercised. Gamma law (nspec 1,
+    O(1) units) or the NASA-7 mixture (nspec 9, CGS) depending on ``eos``."""
+    eos = eos or GammaLaw()
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = (int(e) for e in edges)
+    shp = (nz + 2 * NG, ny + 2 * NG, nx + 2 * NG)
+    jump = np.zeros(shp)
+    if shock:
+        X = np.arange(shp[2])[None, None, :] + 0.7 * np.arange(shp[1])[None, :, None] \
+            + 0.3 * np.arange(shp[0])[:, None, None]
+        jump = (X > 0.5 * X.max()).astype(float)
+    if isinstance(eos, GammaLaw):
+        rho = 1.0 + 0.3 * _smooth_noise(rng, shp) - 0.5 * jump
+        p = 1.0 + 0.3 * _smooth_noise(rng, shp) - 0.7 * jump
+        vel = [0.5 * _smooth_noise(rng, shp) for _ in range(3)]
+        Y = np.ones((1,) + shp)
+    else:
+        T = 1200.0 + 600.0 * _smooth_noise(rng, shp) + 500.0 * jump
+        Y = rng.uniform(0.2, 1.0, size=(eos.nspec,) + shp)
+        Y = Y / Y.sum(axis=0, keepdims=True)
+        p = P_ATM * (1.0 + 0.2 * _smooth_noise(rng, shp) - 0.4 * jump)
+        rho = p / (_rmix(eos, Y) * T)
+        vel = [2.0e4 * _smooth_noise(rng, shp) for _ in range(3)]
+    U = conserved_from_prim(eos, rho, vel[0], vel[1], vel[2], p, Y)
+    dx = (1.0 / 32,) * 3 if isinstance(eos, GammaLaw) else (FLAME_DX,) * 3
+    return Patch((0, 0, 0), (nx - 1, ny - 1, nz - 1), abi.Fab(np.ascontiguousarray(U), (-NG, -NG, -NG)), dx)

@@ -176,6 +176,11 @@ int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* bo
 /* construct_hydro_source over the plan's boxes; dt_dev: DEVICE pointer to the step's
  * dt, or NULL to use each box's dt. */
 int pcg_plan_hydro(pcg_plan* plan, const double* dt_dev, pcg_stream_t stream);
+/* Stages first..last of pcg_plan_hydro only (0 ctoprim, 1 prep, 2 trace, 3 first
+ * Riemann, 4 transverse Riemann, 5 final Riemann and flux adjustment, 6 consup), for
+ * per-stage timing. */
+int pcg_plan_stages(pcg_plan* plan, int32_t first, int32_t last, const double* dt_dev,
+                    pcg_stream_t stream);
 /* cfl * min over the plan's boxes of pc_estdt_hydro, into *dt_dev (DEVICE). */
 int pcg_plan_estdt(pcg_plan* plan, double cfl, double* dt_dev, pcg_stream_t stream);
 /* S_new = S_old + dt * hydro_source in place in each box's uin, then computeTemp. */

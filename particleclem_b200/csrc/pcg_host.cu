@@ -893,6 +893,14 @@ int pcg_plan_hydro(pcg_plan* P, const double* dt_dev, pcg_stream_t stream) {
   return launch_stages(P->L, P->T, &P->prm, K_CTOPRIM, K_CONSUP, dt_dev, reinterpret_cast<cudaStream_t>(stream));
 }
 
+int pcg_plan_stages(pcg_plan* P, int32_t first, int32_t last, const double* dt_dev, pcg_stream_t stream) {
+  if (!P) return fail(PCG_EINVAL, "plan is NULL");
+  if (first < 0 || last >= K_NSTAGE || first > last) return fail(PCG_EINVAL, "stage range %d..%d", first, last);
+  int rc = ensure_eos(P->prm.nspec);
+  if (rc) return rc;
+  return launch_stages(P->L, P->T, &P->prm, first, last, dt_dev, reinterpret_cast<cudaStream_t>(stream));
+}
+
 int pcg_plan_estdt(pcg_plan* P, double cfl, double* dt_dev, pcg_stream_t stream) {
   if (!P || !dt_dev) return fail(PCG_EINVAL, "bad arguments");
   int rc = ensure_eos(P->prm.nspec);

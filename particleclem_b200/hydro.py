@@ -132,6 +132,12 @@ class Plan:
         native.call("pcg_plan_hydro", self.h, C.c_void_p(dt_dev.data_ptr()) if dt_dev is not None else None,
                     _stream_ptr(stream))
 
+    STAGES = ("ctoprim", "prep", "trace", "flux0", "flux1", "flux2", "consup")
+
+    def stages(self, first, last, dt_dev=None, stream=None):
+        native.call("pcg_plan_stages", self.h, int(first), int(last),
+                    C.c_void_p(dt_dev.data_ptr()) if dt_dev is not None else None, _stream_ptr(stream))
+
     def estdt(self, cfl, dt_dev, stream=None):
         native.call("pcg_plan_estdt", self.h, float(cfl), C.c_void_p(dt_dev.data_ptr()), _stream_ptr(stream))
 

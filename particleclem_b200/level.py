@@ -1,0 +1,83 @@
+"""Device-resident single-level advance: the level loop around the hydro path.
+
+One step is what PeleC's level advance does around construct_hydro_source for a
+Godunov run without sources (Source/Advance.cpp:266-352): fill the ghost cells of the
+state (FillPatch/FillBoundary, :307-309), take the CFL timestep of the level
+(estTimeStep, Source/PeleC.cpp:829-960), build the hydro source of every box
+(Source/Hydro.cpp:4-301), then S_new = S_old + dt * hydro_source and computeTemp
+(Source/Advance.cpp:397-417, Source/PeleC.cpp:2289-2305). The state never leaves the
+device, dt stays in device memory, and a step can be captured in a CUDA graph.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import abi, hydro
+
+NG = abi.NGROW
+
+
+class LevelStepper:
+    def __init__(self, level, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, ppm_type=1, plm_iorder=4,
+                 use_flattening=True, difmag=0.1, device=0):
+        import torch
+
+        self.torch = torch
+        self.level = level
+        self.cfl = float(cfl)
+        self.ns = level.nspec
+        self.nv = abi.nvar(self.ns)
+        self.dev = torch.device("cuda", device)
+        hydro.init(device)
+        hydro.set_eos(level.eos)
+        self.state = abi.Fab(torch.from_numpy(np.ascontiguousarray(level.state)).to(self.dev), level.fab.lo)
+        n = [level.domhi[d] - level.domlo[d] + 1 for d in range(3)]
+        self.hsrc = abi.Fab(torch.zeros((self.nv, n[2], n[1], n[0]), dtype=torch.float64, device=self.dev),
+                            tuple(level.domlo))
+        self.dt = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self.prm = abi.make_params(level.dx, 0.0, self.ns, level.domlo, level.domhi, level.bclo, level.bchi,
+                                   ppm_type=ppm_type, plm_iorder=plm_iorder, use_flattening=use_flattening,
+                                   difmag=difmag, precision_mode=precision)
+        self.boxes = [hydro.make_box(lo, hi, self.state, self.hsrc, level.dx, 0.0, level.domlo, level.domhi,
+                                     level.bclo, level.bchi) for lo, hi in level.boxes]
+        self.plan = hydro.Plan(self.prm, self.boxes, fuse=fuse)
+        self.graph = None
+        self.ncells = level.ncells()
+
+    # one level step, enqueued on the current stream
+    def fill(self, stream=None):
+        L = self.level
+        hydro.fill_ghosts(self.state, L.domlo, L.domhi, L.periodic, NG, stream)
+
+    def step(self, stream=None):
+        self.fill(stream)
+        self.plan.estdt(self.cfl, self.dt, stream)
+        self.plan.hydro(self.dt, stream)
+        self.plan.update(self.dt, stream)
+
+    launches_per_step = 3 + 2 + 7 + 1  # fill (3 directions), estdt (2), hydro stages, update
+
+    def capture(self):
+        torch = self.torch
+        s = torch.cuda.Stream(device=self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(s):
+            self.step()  # warm the library (EOS upload, lazy module loading) outside capture
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        torch.cuda.synchronize(self.dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.step()
+        self.graph = g
+        return g
+
+    def replay(self):
+        self.graph.replay()
+
+    def host_state(self):
+        self.torch.cuda.synchronize(self.dev)
+        return self.state.data.cpu().numpy()
+
+    def close(self):
+        self.graph = None
+        self.plan.close()

@@ -62,6 +62,7 @@ SIGNATURES = {
     "pcg_fill_ghosts": ([_A4, _I3, _I3, _I3, C.c_int32, _V], C.c_int),
     "pcg_plan_create": ([_PRM, C.c_int32, _P(Box), C.c_int32, _P(_V)], C.c_int),
     "pcg_plan_hydro": ([_V, _V, _V], C.c_int),
+    "pcg_plan_stages": ([_V, C.c_int32, C.c_int32, _V, _V], C.c_int),
     "pcg_plan_estdt": ([_V, C.c_double, _V, _V], C.c_int),
     "pcg_plan_update": ([_V, _V, _V], C.c_int),
     "pcg_plan_info": ([_V, _P(C.c_int64), _P(C.c_int32), _P(C.c_int64)], C.c_int),

@@ -1,0 +1,53 @@
+"""The C-ABI library: it loads and exports every function include/pcg_hydro.h
+declares, and rejects bad arguments with PCG_E* codes before touching a device."""
+import ctypes as C
+
+import pytest
+
+from particleclem_b200 import abi, native
+
+
+def test_header_declares_the_operator_surface():
+    fns = native.header_functions()
+    for f in ("pcg_ctoprim", "pcg_umdrv", "pcg_hydro_box", "pcg_hydro_boxes", "pcg_estdt", "pcg_update_state",
+              "pcg_fill_ghosts", "pcg_plan_create", "pcg_last_error"):
+        assert f in fns
+
+
+def test_library_exports_every_declared_function():
+    lib = native.load()
+    missing = [f for f in native.header_functions() if not hasattr(lib, f)]
+    assert not missing, missing
+    assert set(native.header_functions()) <= set(native.SIGNATURES), "python binding lags the header"
+
+
+def _rc(name, *args):
+    lib = native.load()
+    return getattr(lib, name)(*args)
+
+
+def test_argument_errors_are_codes_not_aborts():
+    assert _rc("pcg_hydro_box", None, None, None, None, None, None, None) == -1  # PCG_EINVAL
+    assert "params" in native.load().pcg_last_error().decode()
+    assert _rc("pcg_set_eos_gamma", 0.5, 28.97) == -1
+    prm = abi.make_params((1, 1, 1), 0.1, 1, (0, 0, 0), (7, 7, 7), (0, 0, 0), (0, 0, 0), ppm_type=3)
+    assert _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), None, None, None, None) == -1
+    assert "ppm_type" in native.load().pcg_last_error().decode()
+    prm = abi.make_params((1, 1, 1), 0.1, 1, (0, 0, 0), (7, 7, 7), (0, 0, 0), (0, 0, 0))
+    prm.use_hybrid_weno = 1
+    assert _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), None, None, None, None) == -4
+    prm = abi.make_params((1, 1, 1), 0.1, 5, (0, 0, 0), (7, 7, 7), (0, 0, 0), (0, 0, 0))
+    assert _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), None, None, None, None) == -4
+    assert _rc("pcg_plan_destroy", None) == 0
+
+
+@pytest.mark.parametrize("bc", [abi.BC_INFLOW, abi.BC_USER])
+def test_inflow_boundaries_are_reported_unsupported(bc):
+    import numpy as np
+
+    prm = abi.make_params((1, 1, 1), 0.1, 1, (0, 0, 0), (7, 7, 7), (bc, 0, 0), (0, 0, 0))
+    u = abi.Fab(np.zeros((8, 16, 16, 16)), (-4, -4, -4))
+    o = abi.Fab(np.zeros((8, 8, 8, 8)), (0, 0, 0))
+    rc = _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), C.byref(abi.array4(u)),
+             C.byref(abi.array4(o)), None, None)
+    assert rc == -4

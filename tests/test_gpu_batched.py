@@ -1,0 +1,205 @@
+"""GPU tests of the batched form and of the level loop around the hydro path:
+reference golden vectors, uneven box batches, fused levels, multi-step advances with
+the CFL timestep and the temperature Newton solve, CUDA-graph replay, ghost filling."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from common import FP64_TOL, eos9, gpu_zeros, oracle, rel_err, to_cpu, to_gpu
+from particleclem_b200 import abi, hydro, workloads as wl
+from particleclem_b200.level import LevelStepper
+from test_oracle_golden import GOLDEN, load_case
+
+pytestmark = pytest.mark.gpu
+BIG = 1 << 30
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_gpu_fp64_matches_reference_golden(path):
+    z, eos, lo, hi, uin, prm = load_case(path)
+    hydro.init(0)
+    hydro.set_eos(eos)
+    nv = abi.nvar(eos.nspec)
+    g_in = to_gpu(uin)
+    g_out = gpu_zeros(nv, lo, hi)
+    flx = [gpu_zeros(nv, *abi.nodes(lo, hi, d)) for d in range(3)]
+    hydro.hydro_box(prm, lo, hi, g_in, g_out, flx)
+    np.testing.assert_array_equal(to_cpu(g_out), z["hydro_source"])
+    for d in range(3):
+        np.testing.assert_array_equal(to_cpu(flx[d]), z[f"flx{d}"])
+
+
+def _patches(nspec, edges, seed):
+    eos = eos9() if nspec == 9 else None
+    return [wl.random_patch(e, seed + i, eos) for i, e in enumerate(edges)]
+
+
+@pytest.mark.parametrize("nspec", [1, 9])
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_FP64_FAST, abi.PREC_MIXED])
+def test_uneven_batch_equals_single_boxes(nspec, prec):
+    """Boxes of different sizes and dt in one pcg_hydro_boxes call give exactly the
+    per-box results (no cross-box coupling), and the FP64 form equals the oracle."""
+    eos = wl.GammaLaw() if nspec == 1 else eos9()
+    hydro.init(0)
+    hydro.set_eos(eos)
+    o = oracle()
+    o.set_eos(eos)
+    patches = _patches(nspec, [(8, 5, 6), (3, 9, 4), (12, 7, 5), (6, 6, 6)], 40)
+    nv = abi.nvar(nspec)
+    boxes, outs, ins, dts = [], [], [], []
+    for p in patches:
+        dt = (0.2 + 0.1 * len(dts)) * o.estdt(p.lo, p.hi, p.fab, p.dx)
+        dts.append(dt)
+        uin = to_gpu(p.fab)
+        out = gpu_zeros(nv, p.lo, p.hi)
+        ins.append(uin)
+        outs.append(out)
+        boxes.append(hydro.make_box(p.lo, p.hi, uin, out, p.dx, dt))
+    prm = abi.make_params((1, 1, 1), 0.0, nspec, (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), precision_mode=prec)
+    hydro.hydro_boxes(prm, boxes)
+    for p, dt, uin, out in zip(patches, dts, ins, outs):
+        single = gpu_zeros(nv, p.lo, p.hi)
+        prm1 = abi.make_params(p.dx, dt, nspec, (-BIG,) * 3, (BIG,) * 3, (0, 0, 0), (0, 0, 0), precision_mode=prec)
+        hydro.hydro_box(prm1, p.lo, p.hi, uin, single)
+        got = to_cpu(out)
+        np.testing.assert_array_equal(got, to_cpu(single))
+        if prec == abi.PREC_FP64:
+            ref, _ = o.hydro_box(prm1, p.lo, p.hi, p.fab)
+            np.testing.assert_array_equal(got, ref.data)
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_fused_level_equals_per_box(prec):
+    """A level cut into boxes advanced as one fused region gives the per-box results
+    bit for bit (results do not depend on the box decomposition)."""
+    lev = wl.flame(n=24, box=8)
+    hydro.init(0)
+    hydro.set_eos(lev.eos)
+    st_f = LevelStepper(lev, precision=prec, fuse=True)
+    st_b = LevelStepper(lev, precision=prec, fuse=False)
+    assert st_f.plan.info()["nregions"] == 1 and st_b.plan.info()["nregions"] == 27
+    import torch
+
+    dt = torch.full((1,), 2e-8, dtype=torch.float64, device="cuda")
+    st_f.plan.hydro(dt)
+    st_b.plan.hydro(dt)
+    np.testing.assert_array_equal(to_cpu(st_f.hsrc), to_cpu(st_b.hsrc))
+    if prec == abi.PREC_FP64:
+        o = oracle()
+        o.set_eos(lev.eos)
+        prm = abi.make_params(lev.dx, 2e-8, 9, lev.domlo, lev.domhi, lev.bclo, lev.bchi)
+        hs = to_cpu(st_f.hsrc)
+        for lo, hi in lev.boxes[:4]:
+            ref, _ = o.hydro_box(prm, lo, hi, lev.box_fab(lo, hi))
+            sub = hs[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
+            np.testing.assert_array_equal(sub, ref.data)
+    st_f.close()
+    st_b.close()
+
+
+def _oracle_steps(lev, nsteps, cfl=0.3):
+    """The level loop on the CPU oracle: ghost fill, estdt, per-box hydro, update."""
+    o = oracle()
+    o.set_eos(lev.eos)
+    lev = wl.Level(lev.eos, lev.dx, lev.domlo, lev.domhi, lev.bclo, lev.bchi, lev.state.copy(), list(lev.boxes),
+                   lev.periodic)
+    dts = []
+    for _ in range(nsteps):
+        lev.fill_ghosts()
+        fabs = [(lo, hi, lev.box_fab(lo, hi)) for lo, hi in lev.boxes]
+        dt = cfl * min(o.estdt(lo, hi, f, lev.dx) for lo, hi, f in fabs)
+        prm = abi.make_params(lev.dx, dt, lev.nspec, lev.domlo, lev.domhi, lev.bclo, lev.bchi)
+        new = lev.state.copy()
+        g = abi.NGROW
+        for lo, hi, f in fabs:
+            hs, _ = o.hydro_box(prm, lo, hi, f)
+            sn = o.update_state(lo, hi, f, hs, dt)
+            new[:, lo[2] + g:hi[2] + g + 1, lo[1] + g:hi[1] + g + 1, lo[0] + g:hi[0] + g + 1] = sn.view(lo, hi)
+        lev.state = new
+        dts.append(dt)
+    lev.fill_ghosts()
+    return lev.state, dts
+
+
+@pytest.mark.parametrize("name", ["sod", "flame"])
+def test_level_steps_fp64_equal_oracle(name):
+    """Three full level steps (ghost fill, CFL dt on the device, hydro, update with
+    the T(e) Newton solve) in the plain FP64 form equal the oracle's level loop."""
+    lev = wl.sod(16) if name == "sod" else wl.flame(n=16, box=8)
+    ref_state, dts = _oracle_steps(lev, 3)
+    st = LevelStepper(lev, precision=abi.PREC_FP64, fuse=(name == "flame"))
+    got_dts = []
+    for _ in range(3):
+        st.step()
+        got_dts.append(float(st.dt.item()))
+    st.fill()
+    got = st.host_state()
+    assert got_dts == dts
+    np.testing.assert_array_equal(got, ref_state)
+    st.close()
+
+
+def test_graph_replay_equals_eager_steps():
+    lev = wl.flame(n=16, box=8)
+    a = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
+    b = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
+    a.capture()  # the capture warm-up runs one eager step
+    b.step()
+    for _ in range(2):
+        a.replay()
+        b.step()
+    np.testing.assert_array_equal(a.host_state(), b.host_state())
+    a.close()
+    b.close()
+
+
+def test_mixed_level_step_error_vs_fp64():
+    lev = wl.flame(n=32, box=16)
+    a = LevelStepper(lev, precision=abi.PREC_FP64, fuse=False)
+    b = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
+    c = LevelStepper(lev, precision=abi.PREC_FP64_FAST, fuse=True)
+    for s in (a, b, c):
+        s.step()
+    g = abi.NGROW
+    A, B, Cc = (s.host_state()[:, g:-g, g:-g, g:-g] for s in (a, b, c))
+    l1, _ = rel_err(B, A)
+    assert l1 <= 1e-6, l1
+    l1, linf = rel_err(Cc, A)
+    assert l1 <= FP64_TOL and linf <= FP64_TOL, (l1, linf)
+    for s in (a, b, c):
+        s.close()
+
+
+def test_fill_ghosts_matches_numpy():
+    import torch
+
+    lev = wl.turbulence(n=8, box=8, seed=3, kmax=2)
+    s = lev.state.copy()
+    s[:, :4] = -1.0
+    s[:, :, :, -4:] = -2.0
+    st = abi.Fab(torch.from_numpy(s.copy()).cuda(), lev.fab.lo)
+    hydro.init(0)
+    hydro.fill_ghosts(st, lev.domlo, lev.domhi, (True, False, True))
+    wl.fill_ghosts(s, (True, False, True))
+    np.testing.assert_array_equal(to_cpu(st), s)
+
+
+def test_errors_are_reported():
+    from particleclem_b200.native import PcgError
+
+    p = wl.random_patch((4, 4, 4), 1)
+    hydro.init(0)
+    hydro.set_eos(wl.GammaLaw())
+    uin = to_gpu(p.fab)
+    out = gpu_zeros(8, p.lo, p.hi)
+    prm = abi.make_params(p.dx, 1e-3, 1, (-BIG,) * 3, (BIG,) * 3, (0, 0, 0), (0, 0, 0))
+    small = abi.Fab(uin.data[:, 1:-1, 1:-1, 1:-1].contiguous(), (-3, -3, -3))  # only 3 ghosts
+    with pytest.raises(PcgError) as e:
+        hydro.hydro_box(prm, p.lo, p.hi, small, out)
+    assert e.value.code == -1
+    prm.plm_iorder = 3
+    prm.ppm_type = 0
+    with pytest.raises(PcgError):
+        hydro.hydro_box(prm, p.lo, p.hi, uin, out)

@@ -1,0 +1,31 @@
+"""The oracle restatement against the reference's own code on fresh random inputs
+(runs where oracle/_ref was built from the reference checkout)."""
+import numpy as np
+import pytest
+
+import pyoracle
+from common import eos9, oracle
+from particleclem_b200 import abi, workloads as wl
+
+BIG = 1 << 30
+
+
+@pytest.mark.parametrize("seed", [101, 102, 103])
+@pytest.mark.parametrize("nspec", [1, 9])
+@pytest.mark.parametrize("ppm", [1, 0])
+def test_oracle_equals_reference_build(seed, nspec, ppm):
+    if not pyoracle.ref_available(nspec):
+        pytest.skip("oracle/_ref not built (needs the reference checkout)")
+    eos = wl.GammaLaw() if nspec == 1 else eos9()
+    p = wl.random_patch((5, 4, 6), seed, eos if nspec == 9 else None)
+    ref = pyoracle.reference(nspec)
+    ref.set_eos(eos)
+    o = oracle()
+    o.set_eos(eos)
+    dt = 0.3 * ref.estdt(p.lo, p.hi, p.fab, p.dx)
+    prm = abi.make_params(p.dx, dt, nspec, (-BIG,) * 3, (BIG,) * 3, (0, 0, 0), (0, 0, 0), ppm_type=ppm)
+    a, fa = o.hydro_box(prm, p.lo, p.hi, p.fab)
+    b, fb = ref.hydro_box(prm, p.lo, p.hi, p.fab)
+    np.testing.assert_array_equal(a.data, b.data)
+    for d in range(3):
+        np.testing.assert_array_equal(fa[d].data, fb[d].data)

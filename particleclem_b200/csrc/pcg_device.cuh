@@ -35,6 +35,21 @@ template <> struct Lim<float> {
 template <class R> __device__ __forceinline__ R dmin(R a, R b) { return (b < a) ? b : a; }
 template <class R> __device__ __forceinline__ R dmax(R a, R b) { return (a < b) ? b : a; }
 
+// Pressure in the FP32 arithmetic is carried as the deviation p' = p - p0 from a
+// constant p0 of the box (its first cell's pressure): PPM/PLM reconstruction, the
+// characteristic projection, the linearised star state and the flux differences are
+// invariant under a constant pressure shift, so only the EOS calls (which take p0 + p')
+// and the transverse pressure terms (which gain p0 * gamma_c * du) see p0. In FP64 the
+// pressure is absolute (p0 = 0) and these helpers are the identity.
+template <class R> struct PDev { static constexpr bool on = sizeof(R) == 4; };
+template <class R> __device__ __forceinline__ R pabs(R pdev, R p0) {
+  if constexpr (PDev<R>::on) return pdev + p0; else return pdev;
+}
+// floor of the deviation equivalent to the floor f of the absolute pressure
+template <class R> __device__ __forceinline__ R pfloor(R f, R p0) {
+  if constexpr (PDev<R>::on) return f - p0; else return f;
+}
+
 // ------------------------------------------------------------------ views
 template <class T>
 struct V4 {
@@ -170,6 +185,23 @@ struct Eos {
       dpde = (C::gamma() - R(1)) * r;
     } else {
       dpde = r * rm / cv_of(t, y);
+    }
+    dpdr_e = rm * t;
+  }
+  // RTY2P, RTY2Cs, RTY2G and RTY2dpde_dpdre of one state, sharing rmix and cv: each
+  // value is formed by exactly the operations of the separate calls.
+  static __device__ __forceinline__ void rty2all(R r, R t, const R* y, R& p, R& cs, R& g, R& dpde, R& dpdr_e) {
+    const R rm = rmix(y);
+    p = r * rm * t;
+    if (!MIX) {
+      g = C::gamma();
+      cs = sqrt(C::gamma() * p / r);
+      dpde = (C::gamma() - R(1)) * r;
+    } else {
+      const R cv = cv_of(t, y);
+      g = (cv + rm) / cv;
+      cs = sqrt(g * p / r);
+      dpde = r * rm / cv;
     }
     dpdr_e = rm * t;
   }
@@ -383,17 +415,17 @@ struct RiemannOut {
 // sum(rho Y_k e_k(T)).
 template <int NS, bool MIX, class R>
 __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const FaceState<NS, R>& Rs, R cav,
-                                                RiemannOut<R>& o) {
+                                                R p0, RiemannOut<R>& o) {
   using ER = EosR<NS, MIX, R>;
   const R rl = L.rho, ul = L.un, vl = L.ut1, v2l = L.ut2, pl = L.p;
   const R rr = Rs.rho, ur = Rs.un, vr = Rs.ut1, v2r = Rs.ut2, pr = Rs.p;
   const R wsmall = Lim<R>::tiny();
-  const R cl = ER::cs_y(rl, pl, L.y);
-  const R cr = ER::cs_y(rr, pr, Rs.y);
+  const R cl = ER::cs_y(rl, pabs(pl, p0), L.y);
+  const R cr = ER::cs_y(rr, pabs(pr, p0), Rs.y);
   const R wl = dmax(wsmall, cl * rl);
   const R wr = dmax(wsmall, cr * rr);
   const R iwlr = rrcp(wl + wr);
-  const R pstar = dmax(Lim<R>::tiny(), ((wr * pl + wl * pr) + wl * wr * (ul - ur)) * iwlr);
+  const R pstar = dmax(pfloor(Lim<R>::tiny(), p0), ((wr * pl + wl * pr) + wl * wr * (ul - ur)) * iwlr);
   R ustar = ((wl * ul + wr * ur) + (pl - pr)) * iwlr;
   bool mask = ustar > R(0);
   R uo = mask ? ul : ur;
@@ -409,7 +441,7 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
     rspo[n] = mid ? R(0.5) * (rl * L.y[n] + rr * Rs.y[n]) : (mask ? rl * L.y[n] : rr * Rs.y[n]);
     ro += rspo[n];
   }
-  const R co = ER::cs_w(ro, po, rspo);
+  const R co = ER::cs_w(ro, pabs(po, p0), rspo);
   const R drho = rdiv(pstar - po, co * co);
   const R gscale = R(1) + drho * rrcp(ro);
   R rspstar[NS];
@@ -419,7 +451,7 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
     rspstar[n] = dmax(R(0), rspo[n] * gscale);
     rstar += rspstar[n];
   }
-  const R cstar = ER::cs_w(rstar, pstar, rspstar);
+  const R cstar = ER::cs_w(rstar, pabs(pstar, p0), rspstar);
   const R sgnm = copysign(R(1), ustar);
   R spout = co - sgnm * uo;
   R spin = cstar - sgnm * ustar;
@@ -446,7 +478,7 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
     rspo[n] = use_star ? rspstar[n] : use_orig ? rspo[n] : frac * rspstar[n] + (R(1) - frac) * rspo[n];
     rgd += rspo[n];
   }
-  const R regd = ER::rhoe_w(qint_gdpres, rspo);
+  const R regd = ER::rhoe_w(pabs(qint_gdpres, p0), rspo);
   const R frho = rgd * qint_iu;
   o.ustar = ustar;
   o.frho = frho;
@@ -454,7 +486,7 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
   o.fut1 = frho * qint_iv1;
   o.fut2 = frho * qint_iv2;
   const R rhoetot = regd + R(0.5) * rgd * (qint_iu * qint_iu + qint_iv1 * qint_iv1 + qint_iv2 * qint_iv2);
-  o.feden = qint_iu * (rhoetot + qint_gdpres);
+  o.feden = qint_iu * (rhoetot + pabs(qint_gdpres, p0));
   o.feint = qint_iu * regd;
   o.gun = qint_iu;
   o.gpres = qint_gdpres;
@@ -574,7 +606,7 @@ __device__ __forceinline__ void riemann(const FaceState<NS, R>& L, const FaceSta
 // UMY, UMZ, UEDEN, UEINT and the species fluxes in absolute order. DIR is the normal.
 template <int NS, bool MIX, bool EXACT, int DIR, class R>
 __device__ __forceinline__ void cmpflx(const R* ql, const R* qr, int idx, int bclo, int bchi, int domlo, int domhi,
-                                       R cav, R* fl, R& gun, R& gpres) {
+                                       R cav, R p0, R* fl, R& gun, R& gpres) {
   constexpr int t1 = (DIR == 0) ? 1 : 0;
   constexpr int t2 = (DIR == 2) ? 1 : 2;
   FaceState<NS, R> L, Rs;
@@ -610,7 +642,7 @@ __device__ __forceinline__ void cmpflx(const R* ql, const R* qr, int idx, int bc
   if (EXACT)
     riemann<NS, MIX, R>(L, Rs, cav, o);
   else
-    riemann_reduced<NS, MIX, R>(L, Rs, cav, o);
+    riemann_reduced<NS, MIX, R>(L, Rs, cav, p0, o);
   fl[pcg::URHO] = o.frho;
   fl[pcg::UMX + DIR] = o.fun;
   fl[pcg::UMX + t1] = o.fut1;

@@ -56,6 +56,14 @@ __device__ __forceinline__ bool item_of(const pcg::StageArgs& a, Item& it) {
   return true;
 }
 
+// The pressure offset of a region for the FP32 arithmetic (see PDev): the pressure
+// of the region's first valid cell; zero for FP64.
+template <class R>
+__device__ __forceinline__ double p0_of(const pcg::Region& rg) {
+  if constexpr (PDev<R>::on) return v4<const double>(rg.q)(rg.lo[0], rg.lo[1], rg.lo[2], pcg::QPRES);
+  else return 0.0;
+}
+
 // A pointer positioned at one cell of a view: components n at p[n * ns].
 template <class T>
 struct CellPtr {
@@ -108,11 +116,8 @@ __global__ void __launch_bounds__(128) k_ctoprim(pcg::StageArgs a) {
   const double e = (u[pcg::UEDEN] - kineng) * rhoinv;
   const double wbar = E::y2wbar(y);
   const double T = E::rey2t(e, y, u[pcg::UTEMP]);
-  const double p = E::rty2p(rho, T, y);
-  const double cs = E::rty2cs(rho, T, y);
-  const double gam1 = E::rty2g(T, y);
-  double dpde, dpdr_e;
-  E::rty2dpde_dpdre(rho, T, y, dpde, dpdr_e);
+  double p, cs, gam1, dpde, dpdr_e;
+  E::rty2all(rho, T, y, p, cs, gam1, dpde, dpdr_e);
   q[pcg::QTEMP] = T;
   q[pcg::QREINT] = e * rho;
   q[pcg::QPRES] = p;
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
   R flat = R(1);
   if (a.use_flattening) {
 #pragma unroll
-    for (int df = 0; df < 3; df++) flat = dmin(flat, flatten<R>(q, i, j, k, df));
+    for (int df = 0; df < 3; df++) flat = dmin(flat, R(flatten<double>(q, i, j, k, df)));
   }
   R cc;
   if (a.ppm_type == 1) {
@@ -179,10 +184,10 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
 
 // ------------------------------------------------------------------ trace
 template <class R>
-__device__ __forceinline__ void load5(const CellPtr<const double>& c, int64_t st, int n, R* s) {
+__device__ __forceinline__ void load5(const CellPtr<const double>& c, int64_t st, int n, R* s, double off = 0.0) {
   const double* p = c.p + (int64_t)n * c.ns;
 #pragma unroll
-  for (int o = -2; o <= 2; ++o) s[o + 2] = R(p[o * st]);
+  for (int o = -2; o <= 2; ++o) s[o + 2] = PDev<R>::on ? R(p[o * st] - off) : R(p[o * st]);
 }
 
 // Source/PPM.cpp:82-423 for one cell and direction D (bx == vbx as called from
@@ -201,8 +206,10 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
   R Imr[3], Ipr[3], Imu[3], Ipu[3], Imp[3], Ipp[3];
   R Imt[3], Ipt[3];
   const R sp3[3] = {un - cc, un, un + cc};
+  const double p0d = p0_of<R>(rg);
+  const R p0 = R(p0d);
 #define PROFILE3(comp, Im, Ip)                                      \
-  load5<R>(q, st, comp, s);                                          \
+  load5<R>(q, st, comp, s, (comp) == pcg::QPRES ? p0d : 0.0);        \
   ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);    \
   s6 = ppm_s6<R>(sm, sp, s[2]);                                      \
   _Pragma("unroll") for (int w = 0; w < 3; ++w) ppm_wave<R>(sm, sp, s6, sp3[w], dtdx, Ip[w], Im[w]);
@@ -237,8 +244,8 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
     R p_ref = Imp[0];
     rho_ref = dmax(rho_ref, Lim<R>::tiny());
     const R rho_ref_inv = R(1) / rho_ref;
-    p_ref = dmax(p_ref, Lim<R>::tiny());
-    const R cc_ref = EXACT ? E::rpy2cs(rho_ref, p_ref, ym0) : ER::cs_y(rho_ref, p_ref, ym0);
+    p_ref = dmax(p_ref, pfloor(Lim<R>::tiny(), p0));
+    const R cc_ref = EXACT ? E::rpy2cs(rho_ref, p_ref, ym0) : ER::cs_y(rho_ref, pabs(p_ref, p0), ym0);
     const R csq_ref = cc_ref * cc_ref;
     const R cc_ref_inv = R(1) / cc_ref;
     const R dum = un_ref - Imu[0];
@@ -255,14 +262,14 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
     alpha0r = un > R(0) ? R(0) : -alpha0r;
     const R rhos = dmax(Lim<R>::tiny(), rho_ref + alphap + alpham + alpha0r);
     const R uns = un_ref + (alphap - alpham) * cc_ref * rho_ref_inv;
-    const R ps = dmax(Lim<R>::tiny(), p_ref + (alphap + alpham) * csq_ref);
+    const R ps = dmax(pfloor(Lim<R>::tiny(), p0), p_ref + (alphap + alpham) * csq_ref);
     qp[pcg::TR_RHO] = rhos;
 #pragma unroll
     for (int c = 0; c < 3; ++c) qp[pcg::TR_U + c] = (c == D) ? uns : Imt[c];
     qp[pcg::TR_P] = ps;
 #pragma unroll
     for (int n = 0; n < NS; ++n) qp[pcg::TR_Y + n] = ym1[n];
-    qp[pcg::TR_RE] = EXACT ? rhos * E::ryp2e(rhos, ym1, ps) : ER::rhoe_y(rhos, ps, ym1);
+    qp[pcg::TR_RE] = EXACT ? rhos * E::ryp2e(rhos, ym1, ps) : ER::rhoe_y(rhos, pabs(ps, p0), ym1);
   }
   // minus state on face i+1 (Source/PPM.cpp:334-422)
   {
@@ -271,8 +278,8 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
     R p_ref = Ipp[2];
     rho_ref = dmax(rho_ref, Lim<R>::tiny());
     const R rho_ref_inv = R(1) / rho_ref;
-    p_ref = dmax(p_ref, Lim<R>::tiny());
-    const R cc_ref = EXACT ? E::rpy2cs(rho_ref, p_ref, yp2) : ER::cs_y(rho_ref, p_ref, yp2);
+    p_ref = dmax(p_ref, pfloor(Lim<R>::tiny(), p0));
+    const R cc_ref = EXACT ? E::rpy2cs(rho_ref, p_ref, yp2) : ER::cs_y(rho_ref, pabs(p_ref, p0), yp2);
     const R csq_ref = cc_ref * cc_ref;
     const R cc_ref_inv = R(1) / cc_ref;
     const R dum = un_ref - Ipu[0];
@@ -289,14 +296,14 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
     alpha0r = un > R(0) ? -alpha0r : R(0);
     const R rhos = dmax(Lim<R>::tiny(), rho_ref + alphap + alpham + alpha0r);
     const R uns = un_ref + (alphap - alpham) * cc_ref * rho_ref_inv;
-    const R ps = dmax(Lim<R>::tiny(), p_ref + (alphap + alpham) * csq_ref);
+    const R ps = dmax(pfloor(Lim<R>::tiny(), p0), p_ref + (alphap + alpham) * csq_ref);
     qm[pcg::TR_RHO] = rhos;
 #pragma unroll
     for (int c = 0; c < 3; ++c) qm[pcg::TR_U + c] = (c == D) ? uns : Ipt[c];
     qm[pcg::TR_P] = ps;
 #pragma unroll
     for (int n = 0; n < NS; ++n) qm[pcg::TR_Y + n] = yp1[n];
-    qm[pcg::TR_RE] = EXACT ? rhos * E::ryp2e(rhos, yp1, ps) : ER::rhoe_y(rhos, ps, yp1);
+    qm[pcg::TR_RE] = EXACT ? rhos * E::ryp2e(rhos, yp1, ps) : ER::rhoe_y(rhos, pabs(ps, p0), yp1);
   }
 }
 
@@ -310,7 +317,10 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
   const CellPtr<const double> q = at(qv, i, j, k);
   const int64_t st = dstride(qv, D);
   R s[5];
-#define SLOPE(comp) (load5<R>(q, st, comp, s), plm_slope<R>(s[0], s[1], s[2], s[3], s[4], flat, order))
+  const double p0d = p0_of<R>(rg);
+  const R p0 = R(p0d);
+#define SLOPE(comp) (load5<R>(q, st, comp, s, (comp) == pcg::QPRES ? p0d : 0.0), \
+                     plm_slope<R>(s[0], s[1], s[2], s[3], s[4], flat, order))
   const R drho = SLOPE(pcg::QRHO);
   const R dvel[3] = {SLOPE(pcg::QU), SLOPE(pcg::QV), SLOPE(pcg::QW)};
   const R dp = SLOPE(pcg::QPRES);
@@ -319,9 +329,9 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
   const R cs = cc * cc;
   const R rho = R(q[pcg::QRHO]);
   const R vel[3] = {R(q[pcg::QU]), R(q[pcg::QV]), R(q[pcg::QW])};
-  const R p = R(q[pcg::QPRES]);
+  const R p = PDev<R>::on ? R(q[pcg::QPRES] - p0d) : R(q[pcg::QPRES]);
   const R rhoe = R(q[pcg::QREINT]);
-  const R enth = ((rhoe + p) / rho) / cs;
+  const R enth = ((rhoe + pabs(p, p0)) / rho) / cs;
   const R alpham = R(0.5) * (dp / (rho * cc) - dvel[D]) * rho / cc;
   const R alphap = R(0.5) * (dp / (rho * cc) + dvel[D]) * rho / cc;
   const R alpha0r = drho - dp / cs;
@@ -350,7 +360,7 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
     qp[pcg::TR_U + l1] = vel_ref[l1] + azv1rght;
     qp[pcg::TR_U + l2] = vel_ref[l2] + azw1rght;
     r = p_ref + (apright + amright) * cs;
-    qp[pcg::TR_P] = dmax(r, Lim<R>::tiny());
+    qp[pcg::TR_P] = dmax(r, pfloor(Lim<R>::tiny(), p0));
     qp[pcg::TR_RE] = rhoe_ref + (apright + amright) * enth * cs + azeright;
   }
   {
@@ -372,7 +382,7 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
     qm[pcg::TR_U + l1] = vel_ref[l1] + azv1left;
     qm[pcg::TR_U + l2] = vel_ref[l2] + azw1left;
     r = p_ref + (apleft + amleft) * cs;
-    qm[pcg::TR_P] = dmax(r, Lim<R>::tiny());
+    qm[pcg::TR_P] = dmax(r, pfloor(Lim<R>::tiny(), p0));
     qm[pcg::TR_RE] = rhoe_ref + (apleft + amleft) * enth * cs + azeleft;
   }
   const R vel_ad = R(q[pcg::QU + D]);
@@ -426,7 +436,8 @@ __device__ __forceinline__ void face_flux(const pcg::Region& rg, int i, int j, i
   const CellPtr<const double> qa = at(qav, i, j, k);
   const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + (int64_t)pcg::QC * qa.ns]));
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
-  cmpflx<NS, MIX, EXACT, D, R>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav, fl, gun, gpres);
+  cmpflx<NS, MIX, EXACT, D, R>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav,
+                               R(p0_of<R>(rg)), fl, gun, gpres);
 }
 
 template <int NS, class R>
@@ -464,7 +475,7 @@ __global__ void __launch_bounds__(128) k_flux0(pcg::StageArgs a) {
 // O-flux positioned at the cell's low O-face (its high O-face is at +ostride).
 template <int NS, bool EXACT, class R>
 __device__ __forceinline__ void transdo_side(const R* qn, const CellPtr<const R>& f, int64_t ostride, R cdtdx, R c,
-                                             R* out) {
+                                             R p0, R* out) {
   const CellPtr<const R> g = shift(f, ostride);
   const R flxrho = cdtdx * (g[0] - f[0]);
   const R flxu = cdtdx * (g[1] - f[1]);
@@ -504,8 +515,10 @@ __device__ __forceinline__ void transdo_side(const R* qn, const CellPtr<const R>
   const R ke2 = runew * runew + rvnew * rvnew + rwnew * rwnew;
   const R rhoekin = EXACT ? R(0.5) * ke2 / rrnew : R(0.5) * ke2 * irrnew;
   out[pcg::TR_RE] = renew - rhoekin;
-  const R pnew = qn[pcg::TR_P] - cdtdx * (dAup + pav * dAu * (c - R(1)));
-  out[pcg::TR_P] = dmax(pnew, Lim<R>::very_small());
+  R dpt = dAup + pav * dAu * (c - R(1));
+  if constexpr (PDev<R>::on) dpt = dpt + p0 * c * dAu;
+  const R pnew = qn[pcg::TR_P] - cdtdx * dpt;
+  out[pcg::TR_P] = dmax(pnew, pfloor(Lim<R>::very_small(), p0));
 }
 
 // Transverse predictor + paired Riemann solve for the pair (D|O) at D-face (i,j,k)
@@ -518,12 +531,13 @@ __device__ __forceinline__ void flux1_pair(const pcg::StageArgs& a, const pcg::R
   const CellPtr<const R> fo = at(fov, i, j, k);
   const CellPtr<const double> qa = at(qav, i, j, k);
   const R cdt = R(1.0 / 3.0 * dt_of(a, rg) / rg.dx[O]);
+  const R p0 = R(p0_of<R>(rg));
   R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
   load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
   transdo_side<NS, EXACT, R>(qn, shift(fo, -dst_f), ost_f, cdt,
-                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), ql);
+                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), p0, ql);
   load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qn);
-  transdo_side<NS, EXACT, R>(qn, fo, ost_f, cdt, R(qa[pcg::QGAMC]), qr);
+  transdo_side<NS, EXACT, R>(qn, fo, ost_f, cdt, R(qa[pcg::QGAMC]), p0, qr);
   R fl[pcg::nvar(NS)], gun, gpres;
   face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, fl, gun, gpres);
   store_tflux<NS, R>(at(v4<R>(rg.fdo[D][O]), i, j, k), fl, gun, gpres);
@@ -556,7 +570,7 @@ __global__ void __launch_bounds__(128) k_flux1(pcg::StageArgs a) {
 template <int NS, bool EXACT, class R>
 __device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>& fx, int64_t xst,
                                              const CellPtr<const R>& fy, int64_t yst, R cdtdx0, R cdtdx1, R hdt,
-                                             R c, bool has_src, const CellPtr<const double>& sq, R* out) {
+                                             R c, bool has_src, const CellPtr<const double>& sq, R p0, R* out) {
   const CellPtr<const R> gx = shift(fx, xst), gy = shift(fy, yst);
 #define FD(n) (cdtdx0 * (gx[n] - fx[n]) + cdtdx1 * (gy[n] - fy[n]))
   const R flxrho = FD(0);
@@ -582,8 +596,14 @@ __device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>
   const R dAupy = gy[gp] * gy[gu] - fy[gp] * fy[gu];
   const R pavy = R(0.5) * (gy[gp] + fy[gp]);
   const R dAuy = gy[gu] - fy[gu];
-  const R pxnew = cdtdx0 * (dAupx + pavx * dAux * (c - R(1)));
-  const R pynew = cdtdx1 * (dAupy + pavy * dAuy * (c - R(1)));
+  R dptx = dAupx + pavx * dAux * (c - R(1));
+  R dpty = dAupy + pavy * dAuy * (c - R(1));
+  if constexpr (PDev<R>::on) {
+    dptx = dptx + p0 * c * dAux;
+    dpty = dpty + p0 * c * dAuy;
+  }
+  const R pxnew = cdtdx0 * dptx;
+  const R pynew = cdtdx1 * dpty;
   const R s0 = has_src ? R(sq[pcg::QRHO]) : R(0), s1 = has_src ? R(sq[pcg::QU]) : R(0);
   const R s2 = has_src ? R(sq[pcg::QV]) : R(0), s3 = has_src ? R(sq[pcg::QW]) : R(0);
   const R s4 = has_src ? R(sq[pcg::QREINT]) : R(0), s5 = has_src ? R(sq[pcg::QPRES]) : R(0);
@@ -605,7 +625,7 @@ __device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>
   const R rhoekin = EXACT ? R(0.5) * ke2 / rrnew : R(0.5) * ke2 * irrnew;
   out[pcg::TR_RE] = renew - rhoekin + hdt * s4;
   const R pn = qn[pcg::TR_P] - pxnew - pynew + hdt * s5;
-  out[pcg::TR_P] = dmax(pn, Lim<R>::tiny());
+  out[pcg::TR_P] = dmax(pn, pfloor(Lim<R>::tiny(), p0));
 }
 
 // Final fluxes (Source/Godunov.cpp:392-438) followed by the per-face flux adjustments
@@ -626,6 +646,8 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   const R cdtdx0 = R(0.5 * dt / rg.dx[O1]);
   const R cdtdx1 = R(0.5 * dt / rg.dx[O2]);
   const R hdt = R(0.5 * dt);
+  const double p0d = p0_of<R>(rg);
+  const R p0 = R(p0d);
   const bool has_src = rg.srcq.p != nullptr;
   const V4<const double> sqv = v4<const double>(rg.srcq);
   const CellPtr<const double> sqp = has_src ? at(sqv, i, j, k) : CellPtr<const double>{nullptr, 0};
@@ -633,14 +655,15 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
   load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
   transdd_side<NS, EXACT, R>(qn, shift(fx, -xd), xst, shift(fy, -yd), yst, cdtdx0, cdtdx1, hdt,
-                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), has_src, sqm, ql);
+                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), has_src, sqm, p0, ql);
   load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qn);
-  transdd_side<NS, EXACT, R>(qn, fx, xst, fy, yst, cdtdx0, cdtdx1, hdt, R(qa[pcg::QGAMC]), has_src, sqp, qr);
+  transdd_side<NS, EXACT, R>(qn, fx, xst, fy, yst, cdtdx0, cdtdx1, hdt, R(qa[pcg::QGAMC]), has_src, sqp, p0, qr);
   R flr[pcg::nvar(NS)], gun, gpres;
   face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, flr, gun, gpres);
   double fl[pcg::nvar(NS)];
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) fl[n] = (n == pcg::UTEMP) ? 0.0 : double(flr[n]);
+  if constexpr (PDev<R>::on) fl[pcg::UMX + D] += p0d;  // momentum flux back to the absolute pressure
   // pc_artif_visc
   const V4<const double> dv = v4<const double>(rg.divu);
   const int ji = i + (O1 == 0), jj = j + (O1 == 1), jk = k + (O1 == 2);
@@ -675,7 +698,7 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = fl[n] * ar;
   const CellPtr<double> qe = at(v4<double>(rg.qec[D]), i, j, k);
-  qe[0] = double(gpres);
+  qe[0] = PDev<R>::on ? double(gpres) + p0d : double(gpres);
   qe[1] = double(gun);
 }
 

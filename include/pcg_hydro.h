@@ -133,6 +133,21 @@ int pcg_hydro_box(const pcg_hydro_params* prm, const int32_t lo[3], const int32_
                   const pcg_array4* uin, pcg_array4* uout, pcg_array4* flx,
                   pcg_stream_t stream);
 
+/* pcg_hydro_box for callers that must not allocate device memory. No counterpart in
+ * the reference: PeleC's own path allocates its temporaries from the AMReX arena. In a
+ * GPU PeleC run that arena reserves most of the device memory at start-up, so a
+ * plugin's cudaMalloc can fail or fragment what is left, and some hosts forbid the
+ * synchronisation cudaMalloc/cudaFree imply inside their step loop. This entry keeps
+ * its tables and workspace in one 32 MiB static device array of the library and
+ * calls no allocator. Limit: boxes up to 21^3 cells with 9 species or 27^3 with one
+ * species in FP64 (25^3 / 31^3 mixed); larger boxes return PCG_EINVAL. The array's
+ * address is looked up on the first call per device: make that call outside any
+ * stream capture. All calls share the array, so calls that overlap on the GPU
+ * (different streams or unordered host threads) race; calls on one stream do not. */
+int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+                          const pcg_array4* uin, pcg_array4* uout, pcg_array4* flx,
+                          pcg_stream_t stream);
+
 /* ---- batched form -------------------------------------------------------------- */
 
 /* construct_hydro_source over many boxes in one set of launches: every box of the

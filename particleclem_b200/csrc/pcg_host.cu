@@ -956,3 +956,104 @@ int pcg_plan_destroy(pcg_plan* P) {
 }
 
 }  // extern "C"
+
+// ====================================================================== no-allocation entry
+//
+// pcg_hydro_box_noalloc is pcg_hydro_box for callers that must not allocate device
+// memory. Inside a PeleC run the AMReX arena normally reserves most of the GPU's
+// memory up front (amrex.the_arena_init_size), so a plugin's own cudaMalloc can fail or
+// fragment what the arena left; other hosts run under a fixed memory budget or must not
+// take the implicit device synchronisation of cudaMalloc/cudaFree in their step loop.
+// This entry point keeps its launch tables and workspace in one statically sized device
+// array of the library instead.
+//
+// * kNoAllocScratchBytes (32 MiB) is the whole budget: enough for a box of up to 21^3
+//   cells with 9 species or 27^3 with one species in FP64 (25^3 / 31^3 in the mixed
+//   form). Larger boxes are rejected with PCG_EINVAL and a message giving both sizes.
+// * Every GPU that loads the library keeps the 32 MiB array until the process exits.
+// * The array's device address comes from cudaGetSymbolAddress, once per device, on
+//   the first call made with that device current (host code cannot use the symbol
+//   itself: in host code it names a host-side stand-in). Make that first call outside
+//   any stream capture.
+// * All calls share the one array and it keeps the previous call's contents. Nothing in
+//   it has to start at zero: the tables are copied in by each call and every stage
+//   writes each workspace element before a later stage reads it. Calls that overlap on
+//   the GPU (different streams, or different host threads without ordering) race on the
+//   array; calls on one stream are ordered.
+// * Nothing here calls cudaMalloc, cudaMallocAsync, cudaFree or any allocating library
+//   routine. The tables travel with cudaMemcpyAsync from pageable host memory, which
+//   stages them before the call returns.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(PCG_EINVAL, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return fail(PCG_ECUDA, "cudaGetSymbolAddress returned a null address");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return PCG_OK;
+}
+
+}  // namespace
+
+extern "C" int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+                                     const pcg_array4* uin, pcg_array4* uout, pcg_array4* flx,
+                                     pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  if (!lo || !hi || !uin || !uout) return fail(PCG_EINVAL, "lo, hi, uin and uout are required");
+  pcg_box b{};
+  for (int d = 0; d < 3; ++d) {
+    b.lo[d] = lo[d];
+    b.hi[d] = hi[d];
+    b.domlo[d] = prm->domlo[d];
+    b.domhi[d] = prm->domhi[d];
+    b.bclo[d] = prm->bclo[d];
+    b.bchi[d] = prm->bchi[d];
+    b.dx[d] = prm->dx[d];
+  }
+  b.dt = prm->dt;
+  b.uin = *uin;
+  b.uout = *uout;
+  if (flx)
+    for (int d = 0; d < 3; ++d) b.flx[d] = flx[d];
+  std::vector<BoxIn> boxes(1);
+  if ((rc = box_from_desc(b, pcg::nvar(prm->nspec), boxes[0]))) return rc;
+  Layout L;
+  build_layout(L, boxes, prm->nspec, prm->precision_mode == PCG_PREC_MIXED);
+  // scratch = [tables | workspace]; the table size does not depend on the addresses
+  Tables T;
+  pack_tables(L, T);
+  const size_t ws_off = (T.bytes + kAlign - 1) / kAlign * kAlign;
+  const size_t need = ws_off + L.ws_bytes;
+  if (need > kNoAllocScratchBytes)
+    return fail(PCG_EINVAL,
+                "box [%d,%d,%d]-[%d,%d,%d] needs %zu bytes of scratch; pcg_hydro_box_noalloc has %zu "
+                "(use pcg_hydro_box)",
+                lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], need, kNoAllocScratchBytes);
+  if ((rc = ensure_eos(prm->nspec))) return rc;
+  void* base = nullptr;
+  if ((rc = noalloc_scratch(&base))) return rc;
+  char* scratch = static_cast<char*>(base);
+  rebase_workspace(L, boxes, scratch + ws_off);
+  Tables T2;
+  pack_tables(L, T2);  // regions now hold the scratch addresses
+  T2.dev = scratch;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemcpyAsync(T2.dev, T2.host.data(), T2.bytes, cudaMemcpyHostToDevice, s));
+  bind_tables(T2);
+  return launch_stages(L, T2, prm, K_CTOPRIM, K_CONSUP, nullptr, s);
+}

@@ -57,6 +57,7 @@ SIGNATURES = {
     "pcg_umdrv": ([_PRM, _I3, _I3, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _V], C.c_int),
     "pcg_hydro_box": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),
     "pcg_hydro_boxes": ([_PRM, C.c_int32, _P(Box), _V], C.c_int),
+    "pcg_hydro_box_noalloc": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),
     "pcg_estdt": ([C.c_int32, C.c_int32, _P(Box), C.c_double, _V, _V], C.c_int),
     "pcg_update_state": ([C.c_int32, C.c_int32, _P(Box), _A4, _V, _V], C.c_int),
     "pcg_fill_ghosts": ([_A4, _I3, _I3, _I3, C.c_int32, _V], C.c_int),

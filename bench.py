@@ -171,7 +171,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    from particleclem_b200 import abi, hydro, workloads as wl
+    from particleclem_b200 import abi, autotune, hydro, workloads as wl
     from particleclem_b200.level import LevelStepper
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -202,6 +202,8 @@ def run_ours(args):
 
     # ---- headline: batched mixed form, fused plan, one CUDA graph per step
     st = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
+    st.step()  # valid dt and intermediates for the launch-shape autotuner
+    tuned = {"mixed": autotune.tune(st.plan, st.dt, reps=3)}
     st.capture()
     for _ in range(args.warmup):
         st.replay()
@@ -240,6 +242,8 @@ def run_ours(args):
     # ---- plain FP64 drop-in: per-box (reference) semantics, reference operation order
     lev64 = wl.flame(n=args.n, box=args.box, seed=2 + rank)
     st64 = LevelStepper(lev64, precision=abi.PREC_FP64, fuse=False)
+    st64.step()
+    tuned["fp64"] = autotune.tune(st64.plan, st64.dt, reps=3)
     st64.capture()
     st64.replay()
     barrier()
@@ -328,6 +332,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "pinned host state -> H2D -> fill/estdt/hydro/update via C ABI -> D2H, per step"},
             "gpu_launches": LevelStepper.launches_per_step * args.steps,
+            "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},
             "roofline": roof,
             "path_roofline": path_roof,

@@ -204,6 +204,16 @@ int pcg_plan_info(const pcg_plan* plan, int64_t* workspace_bytes, int32_t* nregi
                   int64_t* blocks_per_stage /* [7] */);
 int pcg_plan_destroy(pcg_plan* plan);
 
+/* ---- launch tuning ------------------------------------------------------------- */
+
+/* Each heavy stage (0 ctoprim, 2 trace, 3-5 Riemann stages) exists in three register
+ * budgets (variants 0-2: no cap, moderate, tight); the library keeps the variant used
+ * per (precision_mode, nspec, stage). particleclem_b200/autotune.py times them and
+ * sets the fastest. No counterpart in the reference (AMReX chooses launch shapes). */
+int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage, int32_t variant);
+/* Current variant, or a negative PCG_E* code. */
+int pcg_get_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage);
+
 #ifdef __cplusplus
 }
 #endif

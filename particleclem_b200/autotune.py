@@ -1,0 +1,77 @@
+"""Launch-shape autotuner for the hydro stages.
+
+Every heavy stage (ctoprim, trace, the three Riemann stages) is compiled in three
+register budgets (``kMinBlocks`` in csrc/pcg_kernels.cuh: no cap, moderate, tight),
+which trades registers per thread against resident warps per SM. The best choice
+depends on the precision form (FP32 or FP64 arithmetic), the species count and the GPU,
+so it is measured: :func:`tune` runs each variant of each stage on a live plan with
+CUDA events, keeps the fastest, installs it with ``pcg_set_launch_variant`` and
+returns the table, which :func:`save` / :func:`load` persist as JSON.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+from . import native
+
+TUNED_STAGES = (0, 2, 3, 4, 5)  # ctoprim, trace, flux0, flux1, flux2
+STAGE_NAMES = ("ctoprim", "prep", "trace", "flux0", "flux1", "flux2", "consup")
+NVARIANT = 3
+
+
+def get_variant(prec, nspec, stage):
+    v = native.load().pcg_get_launch_variant(int(prec), int(nspec), int(stage))
+    if v < 0:
+        raise native.PcgError("pcg_get_launch_variant", v, native.load().pcg_last_error().decode())
+    return v
+
+
+def set_variant(prec, nspec, stage, variant):
+    native.call("pcg_set_launch_variant", int(prec), int(nspec), int(stage), int(variant))
+
+
+def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES):
+    """Time every variant of ``stages`` on ``plan`` (a hydro.Plan whose workspace holds
+    a valid state; stages before each tuned one are run once first) and install the
+    fastest. Returns {stage_name: {"variant": v, "ms": [ms per variant]}}."""
+    import torch
+
+    prec, ns = plan.prm.precision_mode, plan.prm.nspec
+    plan.hydro(dt_dev)  # fills every intermediate
+    torch.cuda.synchronize()
+    result = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for st in stages:
+        times = []
+        for v in range(NVARIANT):
+            set_variant(prec, ns, st, v)
+            plan.stages(st, st, dt_dev)  # warm
+            e0.record()
+            for _ in range(reps):
+                plan.stages(st, st, dt_dev)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / reps)
+        best = min(range(NVARIANT), key=lambda v: times[v])
+        set_variant(prec, ns, st, best)
+        result[STAGE_NAMES[st]] = {"variant": best, "ms": [round(t, 4) for t in times]}
+    return result
+
+
+def save(path, prec, nspec, table, gpu_name=None):
+    data = json.load(open(path)) if os.path.exists(path) else {}
+    data[f"prec{prec}_ns{nspec}"] = {"gpu": gpu_name, "stages": table}
+    with open(path, "w") as f:
+        json.dump(data, f, indent=1)
+
+
+def load(path):
+    """Install every table of a JSON file written by :func:`save`."""
+    data = json.load(open(path))
+    for key, entry in data.items():
+        prec = int(key.split("_")[0][4:])
+        ns = int(key.split("_")[1][2:])
+        for name, rec in entry["stages"].items():
+            set_variant(prec, ns, STAGE_NAMES.index(name), rec["variant"])
+    return data

@@ -45,16 +45,20 @@ def up_to_date() -> bool:
     return os.path.exists(LIB) and os.path.getmtime(LIB) >= _sources_mtime()
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, out: str = LIB, extra=()) -> str:
+    """Compile the three translation units and link ``out``. ``extra``: additional nvcc
+    flags for the kernel units (e.g. -DPCG_MINB_FLUX2=4 register caps)."""
+    if not force and out == LIB and up_to_date():
         return LIB
-    os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     cc = nvcc()
+    tag = os.path.basename(out).replace(".so", "")
 
     def compile_unit(item):
-        src, extra = item
-        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
-        cmd = [cc, *COMMON, *ARCH, *extra, "-c", os.path.join(SRC, src), "-o", obj]
+        src, extra_flags = item
+        obj = os.path.join(os.path.dirname(out), tag + "_" + src.replace(".cu", ".o"))
+        flags = list(extra_flags) + (list(extra) if src != "pcg_host.cu" else [])
+        cmd = [cc, *COMMON, *ARCH, *flags, "-c", os.path.join(SRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -64,15 +68,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     with ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
         objs = list(ex.map(compile_unit, UNITS.items()))
-    tmp = LIB + ".tmp"
+    tmp = out + ".tmp"
     cmd = [cc, "-shared", *ARCH, "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB)
+    os.replace(tmp, out)
     for o in objs:
         os.remove(o)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

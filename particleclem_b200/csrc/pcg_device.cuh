@@ -36,7 +36,7 @@ template <class R> __device__ __forceinline__ R dmin(R a, R b) { return (b < a) 
 template <class R> __device__ __forceinline__ R dmax(R a, R b) { return (a < b) ? b : a; }
 
 // Pressure in the FP32 arithmetic is carried as the deviation p' = p - p0 from a
-// constant p0 of the box (its first cell's pressure): PPM/PLM reconstruction, the
+// constant p0 of the box (rho*R/W*T of its first cell): PPM/PLM reconstruction, the
 // characteristic projection, the linearised star state and the flux differences are
 // invariant under a constant pressure shift, so only the EOS calls (which take p0 + p')
 // and the transverse pressure terms (which gain p0 * gamma_c * du) see p0. In FP64 the
@@ -79,6 +79,9 @@ template <> __device__ __forceinline__ float eos_ru<float>() { return (float)pcg
 template <class R, bool MIX> struct EosC;
 template <bool MIX> struct EosC<double, MIX> {
   static __device__ __forceinline__ const pcg::EosConst& e() { return c_eos[MIX ? 1 : 0]; }
+  static __device__ __forceinline__ bool uniform_tmid() { return e().uniform_tmid != 0; }
+  static __device__ __forceinline__ double cvr(int k, int r, int i) { return e().cvc[k][r][i]; }
+  static __device__ __forceinline__ double ecr(int k, int r, int i) { return e().ec[k][r][i]; }
   static __device__ __forceinline__ double gamma() { return e().gamma; }
   static __device__ __forceinline__ double imw(int k) { return e().imw[k]; }
   static __device__ __forceinline__ double tmid(int k) { return e().tmid[k]; }
@@ -87,6 +90,9 @@ template <bool MIX> struct EosC<double, MIX> {
 };
 template <bool MIX> struct EosC<float, MIX> {
   static __device__ __forceinline__ const pcg::EosConst& e() { return c_eos[MIX ? 1 : 0]; }
+  static __device__ __forceinline__ bool uniform_tmid() { return e().uniform_tmid != 0; }
+  static __device__ __forceinline__ float cvr(int k, int r, int i) { return e().cvcf[k][r][i]; }
+  static __device__ __forceinline__ float ecr(int k, int r, int i) { return e().ecf[k][r][i]; }
   static __device__ __forceinline__ float gamma() { return e().gammaf; }
   static __device__ __forceinline__ float imw(int k) { return e().imwf[k]; }
   static __device__ __forceinline__ float tmid(int k) { return e().tmidf[k]; }
@@ -121,13 +127,38 @@ struct Eos {
             c4 = lo ? a[4] : b[4], c5 = lo ? a[5] : b[5];
     return c0 + t * (c1 + t * (c2 + t * (c3 + t * (c4 + t * c5))));
   }
+  // With one range switch temperature for all species the range is chosen once per
+  // call and every coefficient is a compile-time constant-bank operand (no indexed
+  // constant loads); the arithmetic is identical to the per-species selection.
+  template <int RG>
+  static __device__ __forceinline__ R cv_sum(R t, const R* y) {
+    R cv = R(0);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const R cvk = C::cvr(k, RG, 0) + t * (C::cvr(k, RG, 1) + t * (C::cvr(k, RG, 2) + t * (C::cvr(k, RG, 3) + t * C::cvr(k, RG, 4))));
+      cv = cv + y[k] * cvk;
+    }
+    return cv;
+  }
+  template <int RG>
+  static __device__ __forceinline__ R e_sum(R t, const R* y) {
+    R e = R(0);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const R ek = C::ecr(k, RG, 0) + t * (C::ecr(k, RG, 1) + t * (C::ecr(k, RG, 2) + t * (C::ecr(k, RG, 3) + t * (C::ecr(k, RG, 4) + t * C::ecr(k, RG, 5)))));
+      e = e + y[k] * ek;
+    }
+    return e;
+  }
   static __device__ __forceinline__ R cv_of(R t, const R* y) {
+    if (C::uniform_tmid()) return (t < C::tmid(0)) ? cv_sum<0>(t, y) : cv_sum<1>(t, y);
     R cv = R(0);
 #pragma unroll
     for (int k = 0; k < NS; ++k) cv = cv + y[k] * cv_k(k, t);
     return cv;
   }
   static __device__ __forceinline__ R e_of(R t, const R* y) {
+    if (C::uniform_tmid()) return (t < C::tmid(0)) ? e_sum<0>(t, y) : e_sum<1>(t, y);
     R e = R(0);
 #pragma unroll
     for (int k = 0; k < NS; ++k) e = e + y[k] * e_k(k, t);

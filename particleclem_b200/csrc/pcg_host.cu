@@ -23,12 +23,14 @@
 
 namespace pcg_strict {
 cudaError_t upload_eos(int slot, const pcg::EosConst& e);
-cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, cudaStream_t s);
+cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
+                         cudaStream_t s);
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
 }  // namespace pcg_strict
 namespace pcg_fast {
 cudaError_t upload_eos(int slot, const pcg::EosConst& e);
-cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, cudaStream_t s);
+cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
+                         cudaStream_t s);
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
 }  // namespace pcg_fast
 
@@ -40,6 +42,20 @@ constexpr int kThreads = 128;
 constexpr size_t kAlign = 256;
 
 thread_local std::string g_err;
+
+// Launch-variant table: [precision_mode][species slot][stage] -> variant index of
+// kMinBlocks (pcg_kernels.cuh). Defaults measured on B200 for the production flame
+// level; pcg_set_launch_variant (the autotuner) overrides them.
+std::mutex g_var_mu;
+int g_variant[3][2][7] = {
+  {{0, 0, 2, 0, 2, 0, 0}, {2, 0, 1, 1, 1, 1, 0}},  // FP64 reference order
+  {{2, 0, 1, 0, 0, 1, 0}, {2, 0, 1, 0, 0, 1, 0}},  // FP64 with FMA
+  {{0, 0, 2, 0, 2, 2, 0}, {2, 0, 2, 1, 1, 2, 0}},  // mixed
+};
+int variant_of(int prec, int ns, int stage) {
+  std::lock_guard<std::mutex> lk(g_var_mu);
+  return g_variant[prec][ns == 1 ? 0 : 1][stage];
+}
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -250,7 +266,15 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool singl
       R.qa = B.qa;
     }
     take(L, g1, 2, L.esz, R.prep);
-    add_seg(L, K_PREP, (int)r, 0, g1);
+    if (single) {
+      // mixed form: the FP32 primitive copy the trace reads, written by k_ctoprim, or by
+      // k_prep when the caller supplies q (pcg_umdrv)
+      take(L, grow(B.bx, 3), nt, 4, R.qf);
+      R.qf_in_prep = B.internal_q ? 0 : 1;
+      add_seg(L, K_PREP, (int)r, 0, B.internal_q ? g1 : grow(B.bx, 3));
+    } else {
+      add_seg(L, K_PREP, (int)r, 0, g1);
+    }
     take(L, nodes(nodes(nodes(B.bx, 0), 1), 2), 1, 8, R.divu);
     for (int d = 0; d < 3; ++d) {
       IBox tb = g1;
@@ -275,14 +299,17 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool singl
       // one thread per d-face computes both (d|o) pairs that reach it
       add_seg(L, K_FLUX1, (int)r, d, nodes(grow_dir(g1, d, -1), d));
     }
+    // mixed form without flux export: FP32 final fluxes (FP64 accumulation in k_consup)
+    R.ff_single = (single && !B.flx[0].p && !B.flx[1].p && !B.flx[2].p) ? 1 : 0;
+    const size_t fsz = R.ff_single ? 4 : 8;
     for (int d = 0; d < 3; ++d) {
       const IBox fb = nodes(B.bx, d);
       if (B.flx[d].p) {
         R.ff[d] = B.flx[d];
       } else {
-        take(L, fb, nv, 8, R.ff[d]);
+        take(L, fb, nv, fsz, R.ff[d]);
       }
-      take(L, fb, 2, 8, R.qec[d]);
+      take(L, fb, 2, fsz, R.qec[d]);
       add_seg(L, K_FLUX2, (int)r, d, fb);
     }
     add_seg(L, K_CONSUP, (int)r, 0, B.bx);
@@ -300,6 +327,7 @@ void rebase_workspace(Layout& L, const std::vector<BoxIn>& boxes, char* base) {
     const BoxIn& B = boxes[r];
     if (B.internal_q) { rebase(R.q, base); rebase(R.qa, base); }
     rebase(R.prep, base);
+    if (R.qf.p || L.esz == 4) rebase(R.qf, base);
     rebase(R.divu, base);
     for (int d = 0; d < 3; ++d) {
       rebase(R.trm[d], base);
@@ -359,9 +387,10 @@ int launch_stages(const Layout& L, const Tables& T, const pcg_hydro_params* p, i
     a.use_flattening = p->use_flattening;
     a.difmag = p->difmag;
     a.dt_dev = dt_dev;
+    const int var = variant_of(p->precision_mode, L.ns, st);
     cudaError_t e = (p->precision_mode == PCG_PREC_FP64)
-                      ? pcg_strict::launch_stage(st, L.ns, false, a, L.nblocks[st], s)
-                      : pcg_fast::launch_stage(st, L.ns, single, a, L.nblocks[st], s);
+                      ? pcg_strict::launch_stage(st, L.ns, false, a, L.nblocks[st], var, s)
+                      : pcg_fast::launch_stage(st, L.ns, single, a, L.nblocks[st], var, s);
     if (e != cudaSuccess) return fail(PCG_ECUDA, "stage %d launch: %s", st, cudaGetErrorString(e));
   }
   return PCG_OK;
@@ -565,6 +594,9 @@ int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid, const dou
   pcg::EosConst c{};
   c.kind = 1;
   c.nspec = nspec;
+  c.uniform_tmid = 1;
+  for (int k = 1; k < nspec; ++k)
+    if (tmid[k] != tmid[0]) c.uniform_tmid = 0;
   for (int k = 0; k < nspec; ++k) {
     if (!(mw[k] > 0.0)) return fail(PCG_EINVAL, "mw[%d] must be > 0", k);
     const double rw = pcg::RU / mw[k];
@@ -939,6 +971,21 @@ int pcg_plan_info(const pcg_plan* P, int64_t* workspace_bytes, int32_t* nregions
   if (blocks_per_stage)
     for (int s = 0; s < K_NSTAGE; ++s) blocks_per_stage[s] = P->L.nblocks[s];
   return PCG_OK;
+}
+
+int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage, int32_t variant) {
+  if (precision_mode < 0 || precision_mode > 2 || (nspec != 1 && nspec != 9) || stage < 0 || stage >= K_NSTAGE ||
+      variant < 0 || variant > 2)
+    return fail(PCG_EINVAL, "launch variant (%d, %d, %d, %d) out of range", precision_mode, nspec, stage, variant);
+  std::lock_guard<std::mutex> lk(g_var_mu);
+  g_variant[precision_mode][nspec == 1 ? 0 : 1][stage] = variant;
+  return PCG_OK;
+}
+
+int pcg_get_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage) {
+  if (precision_mode < 0 || precision_mode > 2 || (nspec != 1 && nspec != 9) || stage < 0 || stage >= K_NSTAGE)
+    return fail(PCG_EINVAL, "launch variant query out of range");
+  return variant_of(precision_mode, nspec, stage);
 }
 
 int pcg_plan_destroy(pcg_plan* P) {

@@ -25,6 +25,19 @@ namespace PCG_TU {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
 
+// Launch variants: each heavy stage is compiled with a few minimum-resident-blocks
+// requests (__launch_bounds__ register caps); the host picks one per (form, species
+// count, stage) from a table the autotuner fills. 0 = no cap.
+constexpr int kMinBlocks[K_NSTAGE][3] = {
+  {0, 3, 5},  // ctoprim
+  {0, 0, 0},  // prep
+  {0, 4, 5},  // trace
+  {0, 6, 8},  // flux0
+  {0, 6, 8},  // flux1
+  {0, 4, 5},  // flux2
+  {0, 0, 0},  // consup
+};
+
 struct Item {
   const pcg::Region* rg;
   int variant;
@@ -56,14 +69,6 @@ __device__ __forceinline__ bool item_of(const pcg::StageArgs& a, Item& it) {
   return true;
 }
 
-// The pressure offset of a region for the FP32 arithmetic (see PDev): the pressure
-// of the region's first valid cell; zero for FP64.
-template <class R>
-__device__ __forceinline__ double p0_of(const pcg::Region& rg) {
-  if constexpr (PDev<R>::on) return v4<const double>(rg.q)(rg.lo[0], rg.lo[1], rg.lo[2], pcg::QPRES);
-  else return 0.0;
-}
-
 // A pointer positioned at one cell of a view: components n at p[n * ns].
 template <class T>
 struct CellPtr {
@@ -84,10 +89,28 @@ __device__ __forceinline__ int64_t dstride(const V4<T>& v, int d) {
   return d == 0 ? 1 : d == 1 ? v.js : v.ks;
 }
 
+// The pressure offset of a region for the FP32 arithmetic (see PDev): rho * rmix * T of
+// the region's first valid cell, from the conserved state and its stored temperature
+// (any constant of the region would do; this one needs no neighbour and no Newton
+// solve, so every stage computes the same value); zero for FP64.
+template <int NS, bool MIX, class R>
+__device__ __forceinline__ double p0_of(const pcg::Region& rg) {
+  if constexpr (PDev<R>::on) {
+    const CellPtr<const double> u{&v4<const double>(rg.uin)(rg.lo[0], rg.lo[1], rg.lo[2], 0), rg.uin.ns};
+    const double rho = u[pcg::URHO];
+    double y[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) y[n] = u[pcg::UFS + n] / rho;
+    return rho * Eos<NS, MIX, double>::rmix(y) * u[pcg::UTEMP];
+  } else {
+    return 0.0;
+  }
+}
+
 // ------------------------------------------------------------------ ctoprim
 // Source/PeleCUtilities.H:242-320 (pc_ctoprim), omega = rad = 0.
-template <int NS, bool MIX>
-__global__ void __launch_bounds__(128) k_ctoprim(pcg::StageArgs a) {
+template <int NS, bool MIX, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_ctoprim(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   const pcg::Region& rg = *it.rg;
@@ -128,6 +151,20 @@ __global__ void __launch_bounds__(128) k_ctoprim(pcg::StageArgs a) {
   qa[pcg::QC] = cs;
   qa[pcg::QCSML] = dmax(pcg::SMALL_NUM, pcg::SMALL_NUM * cs);
   qa[pcg::QRSPEC] = pcg::RU / wbar;
+  // mixed form: the FP32 primitive copy the trace reads, on grow(box,3)
+  if (rg.qf.p && !rg.qf_in_prep && it.i >= rg.lo[0] - 3 && it.i <= rg.hi[0] + 3 && it.j >= rg.lo[1] - 3 &&
+      it.j <= rg.hi[1] + 3 && it.k >= rg.lo[2] - 3 && it.k <= rg.hi[2] + 3) {
+    const double p0 = p0_of<NS, MIX, float>(rg);
+    const CellPtr<float> f = at(v4<float>(rg.qf), it.i, it.j, it.k);
+    f[pcg::TR_RHO] = float(rho);
+    f[pcg::TR_U] = float(vx);
+    f[pcg::TR_V] = float(vy);
+    f[pcg::TR_W] = float(vz);
+    f[pcg::TR_P] = float(p - p0);
+    f[pcg::TR_RE] = float(e * rho);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) f[pcg::TR_Y + n] = float(y[n]);
+  }
 }
 
 // ------------------------------------------------------------------ prep
@@ -160,6 +197,24 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
   const pcg::Region& rg = *it.rg;
   const int i = it.i, j = it.j, k = it.k;
   const V4<const double> q = v4<const double>(rg.q);
+  if constexpr (PDev<R>::on) if (rg.qf_in_prep) {
+    // FP32 copy of the primitive state for the trace (grow(box,3)), when the caller
+    // supplied q (pcg_umdrv) and no ctoprim stage runs
+    const double p0 = p0_of<NS, MIX, R>(rg);
+    const CellPtr<const double> qc = at(q, i, j, k);
+    const CellPtr<float> f = at(v4<float>(rg.qf), i, j, k);
+    f[pcg::TR_RHO] = float(qc[pcg::QRHO]);
+    f[pcg::TR_U] = float(qc[pcg::QU]);
+    f[pcg::TR_V] = float(qc[pcg::QV]);
+    f[pcg::TR_W] = float(qc[pcg::QW]);
+    f[pcg::TR_P] = float(qc[pcg::QPRES] - p0);
+    f[pcg::TR_RE] = float(qc[pcg::QREINT]);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) f[pcg::TR_Y + n] = float(qc[pcg::QFS + n]);
+  }
+  const bool in_g1 = i >= rg.lo[0] - 1 && i <= rg.hi[0] + 1 && j >= rg.lo[1] - 1 && j <= rg.hi[1] + 1 &&
+                     k >= rg.lo[2] - 1 && k <= rg.hi[2] + 1;
+  if (!in_g1) return;
   R flat = R(1);
   if (a.use_flattening) {
 #pragma unroll
@@ -183,12 +238,49 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
 }
 
 // ------------------------------------------------------------------ trace
-template <class R>
-__device__ __forceinline__ void load5(const CellPtr<const double>& c, int64_t st, int n, R* s, double off = 0.0) {
-  const double* p = c.p + (int64_t)n * c.ns;
-#pragma unroll
-  for (int o = -2; o <= 2; ++o) s[o + 2] = PDev<R>::on ? R(p[o * st] - off) : R(p[o * st]);
+// The primitive state the trace reads: q itself (double, QVAR layout) in the FP64
+// forms; in the mixed form the FP32 copy qf written by k_prep (trace-state layout,
+// pressure as the deviation from the box's p0), so no conversions are left in the trace.
+__device__ __forceinline__ int tr_comp(int qcomp) {
+  return qcomp == pcg::QRHO ? pcg::TR_RHO
+         : qcomp <= pcg::QW ? pcg::TR_U + (qcomp - pcg::QU)
+         : qcomp == pcg::QPRES ? pcg::TR_P
+         : qcomp == pcg::QREINT ? pcg::TR_RE
+                                : pcg::TR_Y + (qcomp - pcg::QFS);
 }
+template <class R> struct Prim;
+template <> struct Prim<double> {
+  const double* p;
+  int64_t ns, st;
+  __device__ __forceinline__ Prim(const pcg::Region& rg, int i, int j, int k, int d) {
+    const V4<const double> v = v4<const double>(rg.q);
+    p = &v(i, j, k, 0);
+    ns = v.ns;
+    st = dstride(v, d);
+  }
+  __device__ __forceinline__ double c(int qcomp) const { return p[qcomp * ns]; }
+  __device__ __forceinline__ void five(int qcomp, double* s) const {
+    const double* b = p + qcomp * ns;
+#pragma unroll
+    for (int o = -2; o <= 2; ++o) s[o + 2] = b[o * st];
+  }
+};
+template <> struct Prim<float> {
+  const float* p;
+  int64_t ns, st;
+  __device__ __forceinline__ Prim(const pcg::Region& rg, int i, int j, int k, int d) {
+    const V4<const float> v = v4<const float>(rg.qf);
+    p = &v(i, j, k, 0);
+    ns = v.ns;
+    st = dstride(v, d);
+  }
+  __device__ __forceinline__ float c(int qcomp) const { return p[tr_comp(qcomp) * ns]; }
+  __device__ __forceinline__ void five(int qcomp, float* s) const {
+    const float* b = p + tr_comp(qcomp) * ns;
+#pragma unroll
+    for (int o = -2; o <= 2; ++o) s[o + 2] = b[o * st];
+  }
+};
 
 // Source/PPM.cpp:82-423 for one cell and direction D (bx == vbx as called from
 // Source/Godunov.cpp:188-200, so both states are produced). Only the components the
@@ -197,19 +289,16 @@ template <int NS, bool MIX, bool EXACT, int D, class R>
 __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, double dt) {
   using E = Eos<NS, MIX, R>;
   using ER = EosR<NS, MIX, R>;
-  const V4<const double> qv = v4<const double>(rg.q);
-  const CellPtr<const double> q = at(qv, i, j, k);
-  const int64_t st = dstride(qv, D);
+  const Prim<R> P(rg, i, j, k, D);
   const R dtdx = R(dt / rg.dx[D]);
-  const R un = R(q[pcg::QU + D]);
+  const R un = P.c(pcg::QU + D);
   R s[5], sm, sp, s6;
   R Imr[3], Ipr[3], Imu[3], Ipu[3], Imp[3], Ipp[3];
   R Imt[3], Ipt[3];
   const R sp3[3] = {un - cc, un, un + cc};
-  const double p0d = p0_of<R>(rg);
-  const R p0 = R(p0d);
+  const R p0 = R(p0_of<NS, MIX, R>(rg));
 #define PROFILE3(comp, Im, Ip)                                      \
-  load5<R>(q, st, comp, s, (comp) == pcg::QPRES ? p0d : 0.0);        \
+  P.five(comp, s);                                                   \
   ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);    \
   s6 = ppm_s6<R>(sm, sp, s[2]);                                      \
   _Pragma("unroll") for (int w = 0; w < 3; ++w) ppm_wave<R>(sm, sp, s6, sp3[w], dtdx, Ip[w], Im[w]);
@@ -219,7 +308,7 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (c == D) continue;
-    load5<R>(q, st, pcg::QU + c, s);
+    P.five(pcg::QU + c, s);
     ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);
     s6 = ppm_s6<R>(sm, sp, s[2]);
     ppm_wave<R>(sm, sp, s6, un, dtdx, Ipt[c], Imt[c]);
@@ -308,29 +397,25 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
 }
 
 // Source/PLM.H:167-309 (pc_plm_d) with the slopes of Source/Godunov.cpp:139-180.
-template <int NS, int D, class R>
+template <int NS, bool MIX, int D, class R>
 __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
                                               double dt) {
   constexpr int l1 = (D == 0) ? 1 : 0;
   constexpr int l2 = (D == 2) ? 1 : 2;
-  const V4<const double> qv = v4<const double>(rg.q);
-  const CellPtr<const double> q = at(qv, i, j, k);
-  const int64_t st = dstride(qv, D);
+  const Prim<R> P(rg, i, j, k, D);
   R s[5];
-  const double p0d = p0_of<R>(rg);
-  const R p0 = R(p0d);
-#define SLOPE(comp) (load5<R>(q, st, comp, s, (comp) == pcg::QPRES ? p0d : 0.0), \
-                     plm_slope<R>(s[0], s[1], s[2], s[3], s[4], flat, order))
+  const R p0 = R(p0_of<NS, MIX, R>(rg));
+#define SLOPE(comp) (P.five(comp, s), plm_slope<R>(s[0], s[1], s[2], s[3], s[4], flat, order))
   const R drho = SLOPE(pcg::QRHO);
   const R dvel[3] = {SLOPE(pcg::QU), SLOPE(pcg::QV), SLOPE(pcg::QW)};
   const R dp = SLOPE(pcg::QPRES);
   const R drhoe = SLOPE(pcg::QREINT);
   const R dtdx = R(dt / rg.dx[D]);
   const R cs = cc * cc;
-  const R rho = R(q[pcg::QRHO]);
-  const R vel[3] = {R(q[pcg::QU]), R(q[pcg::QV]), R(q[pcg::QW])};
-  const R p = PDev<R>::on ? R(q[pcg::QPRES] - p0d) : R(q[pcg::QPRES]);
-  const R rhoe = R(q[pcg::QREINT]);
+  const R rho = P.c(pcg::QRHO);
+  const R vel[3] = {P.c(pcg::QU), P.c(pcg::QV), P.c(pcg::QW)};
+  const R p = P.c(pcg::QPRES);
+  const R rhoe = P.c(pcg::QREINT);
   const R enth = ((rhoe + pabs(p, p0)) / rho) / cs;
   const R alpham = R(0.5) * (dp / (rho * cc) - dvel[D]) * rho / cc;
   const R alphap = R(0.5) * (dp / (rho * cc) + dvel[D]) * rho / cc;
@@ -385,13 +470,13 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
     qm[pcg::TR_P] = dmax(r, pfloor(Lim<R>::tiny(), p0));
     qm[pcg::TR_RE] = rhoe_ref + (apleft + amleft) * enth * cs + azeleft;
   }
-  const R vel_ad = R(q[pcg::QU + D]);
+  const R vel_ad = P.c(pcg::QU + D);
   const R spzerom = (vel_ad > R(0)) ? R(-1) : vel_ad * dtdx;
   const R spzerop = (vel_ad >= R(0)) ? vel_ad * dtdx : R(1);
 #pragma unroll
   for (int n = 0; n < NS; n++) {
     const R slope = SLOPE(pcg::QFS + n);
-    const R qc = R(q[pcg::QFS + n]);
+    const R qc = P.c(pcg::QFS + n);
     const R acmprght = R(0.5) * (R(-1) - spzerom) * slope;
     qp[pcg::TR_Y + n] = qc + acmprght;
     const R acmpleft = R(0.5) * (R(1) - spzerop) * slope;
@@ -408,11 +493,11 @@ __device__ __forceinline__ void trace_cell(const pcg::StageArgs& a, const pcg::R
   if (a.ppm_type == 1)
     trace_ppm_dir<NS, MIX, EXACT, D, R>(rg, i, j, k, cc, flat, dt);
   else
-    trace_plm_dir<NS, D, R>(rg, i, j, k, cc, flat, a.plm_iorder, dt);
+    trace_plm_dir<NS, MIX, D, R>(rg, i, j, k, cc, flat, a.plm_iorder, dt);
 }
 
-template <int NS, bool MIX, bool EXACT, class R>
-__global__ void __launch_bounds__(128) k_trace(pcg::StageArgs a) {
+template <int NS, bool MIX, bool EXACT, class R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_trace(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   switch (it.variant) {
@@ -437,7 +522,7 @@ __device__ __forceinline__ void face_flux(const pcg::Region& rg, int i, int j, i
   const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + (int64_t)pcg::QC * qa.ns]));
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
   cmpflx<NS, MIX, EXACT, D, R>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav,
-                               R(p0_of<R>(rg)), fl, gun, gpres);
+                               R(p0_of<NS, MIX, R>(rg)), fl, gun, gpres);
 }
 
 template <int NS, class R>
@@ -460,8 +545,8 @@ __device__ __forceinline__ void flux0_face(const pcg::Region& rg, int i, int j, 
   store_tflux<NS, R>(at(v4<R>(rg.fi[D]), i, j, k), fl, gun, gpres);
 }
 
-template <int NS, bool MIX, bool EXACT, class R>
-__global__ void __launch_bounds__(128) k_flux0(pcg::StageArgs a) {
+template <int NS, bool MIX, bool EXACT, class R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_flux0(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   switch (it.variant) {
@@ -531,7 +616,7 @@ __device__ __forceinline__ void flux1_pair(const pcg::StageArgs& a, const pcg::R
   const CellPtr<const R> fo = at(fov, i, j, k);
   const CellPtr<const double> qa = at(qav, i, j, k);
   const R cdt = R(1.0 / 3.0 * dt_of(a, rg) / rg.dx[O]);
-  const R p0 = R(p0_of<R>(rg));
+  const R p0 = R(p0_of<NS, MIX, R>(rg));
   R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
   load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
   transdo_side<NS, EXACT, R>(qn, shift(fo, -dst_f), ost_f, cdt,
@@ -553,8 +638,8 @@ __device__ __forceinline__ void flux1_face(const pcg::StageArgs& a, const pcg::R
   if (c[O2] >= rg.lo[O2] && c[O2] <= rg.hi[O2]) flux1_pair<NS, MIX, EXACT, D, O2, R>(a, rg, i, j, k);
 }
 
-template <int NS, bool MIX, bool EXACT, class R>
-__global__ void __launch_bounds__(128) k_flux1(pcg::StageArgs a) {
+template <int NS, bool MIX, bool EXACT, class R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_flux1(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   switch (it.variant) {
@@ -646,7 +731,7 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   const R cdtdx0 = R(0.5 * dt / rg.dx[O1]);
   const R cdtdx1 = R(0.5 * dt / rg.dx[O2]);
   const R hdt = R(0.5 * dt);
-  const double p0d = p0_of<R>(rg);
+  const double p0d = p0_of<NS, MIX, R>(rg);
   const R p0 = R(p0d);
   const bool has_src = rg.srcq.p != nullptr;
   const V4<const double> sqv = v4<const double>(rg.srcq);
@@ -694,6 +779,18 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) fl[n] *= fac;
   // pc_ext_flx
   const double ar = rg.area[D].p ? v4<const double>(rg.area[D])(i, j, k) : rg.area_u[D];
+  if (PDev<R>::on && rg.ff_single) {
+    // FP32 final fluxes for the FP64 divergence accumulation, normal momentum flux and
+    // Godunov pressure as deviations from p0 (the divergence is shift invariant)
+    fl[pcg::UMX + D] -= p0d;
+    const CellPtr<float> ff = at(v4<float>(rg.ff[D]), i, j, k);
+#pragma unroll
+    for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = float(fl[n] * ar);
+    const CellPtr<float> qe = at(v4<float>(rg.qec[D]), i, j, k);
+    qe[0] = float(gpres);
+    qe[1] = float(gun);
+    return;
+  }
   const CellPtr<double> ff = at(v4<double>(rg.ff[D]), i, j, k);
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = fl[n] * ar;
@@ -702,8 +799,8 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   qe[1] = double(gun);
 }
 
-template <int NS, bool MIX, bool EXACT, class R>
-__global__ void __launch_bounds__(128) k_flux2(pcg::StageArgs a) {
+template <int NS, bool MIX, bool EXACT, class R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   switch (it.variant) {
@@ -713,21 +810,18 @@ __global__ void __launch_bounds__(128) k_flux2(pcg::StageArgs a) {
   }
 }
 
-// Source/Godunov.H:1033-1060 (pc_pdivu) and Source/Hydro.H:888-907 (pc_update).
-template <int NS>
-__global__ void __launch_bounds__(128) k_consup(pcg::StageArgs a) {
-  Item it;
-  if (!item_of(a, it)) return;
-  const pcg::Region& rg = *it.rg;
-  const int i = it.i, j = it.j, k = it.k;
-  const V4<const double> f0v = v4<const double>(rg.ff[0]), f1v = v4<const double>(rg.ff[1]),
-                         f2v = v4<const double>(rg.ff[2]);
-  const CellPtr<const double> f0 = at(f0v, i, j, k), f1 = at(f1v, i, j, k), f2 = at(f2v, i, j, k);
-  const CellPtr<const double> f0p = shift(f0, 1), f1p = shift(f1, f1v.js), f2p = shift(f2, f2v.ks);
-  const V4<const double> q0v = v4<const double>(rg.qec[0]), q1v = v4<const double>(rg.qec[1]),
-                         q2v = v4<const double>(rg.qec[2]);
-  const CellPtr<const double> q0 = at(q0v, i, j, k), q1 = at(q1v, i, j, k), q2 = at(q2v, i, j, k);
-  const CellPtr<const double> q0p = shift(q0, 1), q1p = shift(q1, q1v.js), q2p = shift(q2, q2v.ks);
+// Source/Godunov.H:1033-1060 (pc_pdivu) and Source/Hydro.H:888-907 (pc_update), FP64
+// accumulation. F is the element type of the final fluxes (double, or float with the
+// pressure as deviation from p0; p0 cancels in the flux differences and is added back to
+// the Godunov pressures of pdivu).
+template <int NS, class F>
+__device__ __forceinline__ void consup_cell(const pcg::Region& rg, int i, int j, int k, double p0) {
+  const V4<const F> f0v = v4<const F>(rg.ff[0]), f1v = v4<const F>(rg.ff[1]), f2v = v4<const F>(rg.ff[2]);
+  const CellPtr<const F> f0 = at(f0v, i, j, k), f1 = at(f1v, i, j, k), f2 = at(f2v, i, j, k);
+  const CellPtr<const F> f0p = shift(f0, 1), f1p = shift(f1, f1v.js), f2p = shift(f2, f2v.ks);
+  const V4<const F> q0v = v4<const F>(rg.qec[0]), q1v = v4<const F>(rg.qec[1]), q2v = v4<const F>(rg.qec[2]);
+  const CellPtr<const F> q0 = at(q0v, i, j, k), q1 = at(q1v, i, j, k), q2 = at(q2v, i, j, k);
+  const CellPtr<const F> q0p = shift(q0, 1), q1p = shift(q1, q1v.js), q2p = shift(q2, q2v.ks);
   const bool ua = rg.area[0].p != nullptr;
   const V4<const double> a0 = v4<const double>(rg.area[0]);
   const V4<const double> a1 = v4<const double>(rg.area[1]);
@@ -737,17 +831,30 @@ __global__ void __launch_bounds__(128) k_consup(pcg::StageArgs a) {
   const double a2m = ua ? a2(i, j, k) : rg.area_u[2], a2p = ua ? a2(i, j, k + 1) : rg.area_u[2];
   const double v = rg.vol.p ? v4<const double>(rg.vol)(i, j, k) : rg.vol_u;
   const double pdivu = 0.5 *
-                       ((q0p[0] + q0[0]) * (q0p[1] * a0p - q0[1] * a0m) +
-                        (q1p[0] + q1[0]) * (q1p[1] * a1p - q1[1] * a1m) +
-                        (q2p[0] + q2[0]) * (q2p[1] * a2p - q2[1] * a2m)) /
+                       ((double(q0p[0]) + p0 + (double(q0[0]) + p0)) * (double(q0p[1]) * a0p - double(q0[1]) * a0m) +
+                        (double(q1p[0]) + p0 + (double(q1[0]) + p0)) * (double(q1p[1]) * a1p - double(q1[1]) * a1m) +
+                        (double(q2p[0]) + p0 + (double(q2[0]) + p0)) * (double(q2p[1]) * a2p - double(q2[1]) * a2m)) /
                        v;
   const CellPtr<double> uo = at(v4<double>(rg.uout), i, j, k);
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) {
     const double old = rg.zero_uout ? 0.0 : uo[n];
-    uo[n] = old + (f0[n] - f0p[n] + f1[n] - f1p[n] + f2[n] - f2p[n]) / v;
+    uo[n] = old + (double(f0[n]) - double(f0p[n]) + double(f1[n]) - double(f1p[n]) + double(f2[n]) -
+                   double(f2p[n])) /
+                      v;
   }
   uo[pcg::UEINT] -= pdivu;
+}
+
+template <int NS, bool MIX>
+__global__ void __launch_bounds__(128) k_consup(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  const pcg::Region& rg = *it.rg;
+  if (rg.ff_single)
+    consup_cell<NS, float>(rg, it.i, it.j, it.k, p0_of<NS, MIX, float>(rg));
+  else
+    consup_cell<NS, double>(rg, it.i, it.j, it.k, 0.0);
 }
 
 }  // namespace PCG_TU

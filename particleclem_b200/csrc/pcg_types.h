@@ -44,6 +44,7 @@ constexpr int MAXNS = 16;
 struct EosConst {
   int kind;  // 0 gamma law, 1 NASA-7 mixture
   int nspec;
+  int uniform_tmid;  // 1: every species switches NASA-7 range at tmid[0]
   double gamma;
   double imw[MAXNS];
   double tmid[MAXNS];
@@ -80,6 +81,8 @@ struct Region {
   View qa;          // auxiliary state, double, NQAUX comps
   View srcq;        // primitive sources (p == nullptr: none)
   View prep;        // flattening and trace sound speed on grow(box,1), compute type
+  View qf;          // mixed form: FP32 copy of q on grow(box,3) in trace-state layout
+                    // (rho, u, v, w, p - p0, rho e, Y), p == nullptr otherwise
   View divu;        // nodal div u on the box's nodes, double
   View area[3];     // face areas (p == nullptr: uniform)
   View vol;         // cell volumes (p == nullptr: uniform)
@@ -90,7 +93,9 @@ struct Region {
   View ff[3];       // final fluxes, double, NVAR comps (area-weighted)
   View qec[3];      // Godunov pressure and normal velocity at final faces, double
   int32_t zero_uout; // 1: write uout (=), 0: accumulate (+=)
-  int32_t pad;
+  int32_t qf_in_prep; // 1: k_prep writes qf (no ctoprim stage), 0: k_ctoprim writes it
+  int32_t ff_single;  // 1: ff/qec are FP32 with the pressure as deviation from p0
+  int32_t pad2;
 };
 
 // A run of thread blocks of one stage working on one region (and one variant, e.g.

@@ -68,6 +68,8 @@ SIGNATURES = {
     "pcg_plan_update": ([_V, _V, _V], C.c_int),
     "pcg_plan_info": ([_V, _P(C.c_int64), _P(C.c_int32), _P(C.c_int64)], C.c_int),
     "pcg_plan_destroy": ([_V], C.c_int),
+    "pcg_set_launch_variant": ([C.c_int32, C.c_int32, C.c_int32, C.c_int32], C.c_int),
+    "pcg_get_launch_variant": ([C.c_int32, C.c_int32, C.c_int32], C.c_int),
 }
 
 _lib = None
@@ -82,8 +84,10 @@ def header_functions(path: str = HEADER):
 
 
 def lib_path() -> str:
+    """The library to load: PCG_LIB if set (an alternative build, e.g. from the
+    launch-shape tuner), else the in-tree build."""
     from .build import LIB
-    return LIB
+    return os.environ.get("PCG_LIB", LIB)
 
 
 def load(build_if_missing: bool = True):
@@ -94,7 +98,7 @@ def load(build_if_missing: bool = True):
             return _lib
         path = lib_path()
         if not os.path.exists(path):
-            if not build_if_missing:
+            if not build_if_missing or "PCG_LIB" in os.environ:
                 raise OSError(f"{path} is missing; run particleclem_b200/build.py")
             from .build import build
             build()

@@ -5,7 +5,8 @@ it reads and every output element it writes, each counted once per launch (no st
 re-reads). For a region of valid edges (nx, ny, nz), NS species, compute-type size
 ``r`` (8 FP64, 4 mixed) and NT = 6 + NS, NF = 7 + NS, NVAR = 7 + NS, QVAR = 8 + NS:
 
-* ctoprim: read NVAR doubles and write QVAR + 6 doubles per cell of grow(box, 4)
+* ctoprim: read NVAR doubles and write QVAR + 6 doubles per cell of grow(box, 4); the
+           mixed form (r = 4) also writes the FP32 copy of NT primitives on grow(box, 3)
 * prep:    read (5 + NS) q doubles per cell of grow(box, 4); write 2 r per cell of
            grow(box, 1) and one double per node of the box
 * trace:   read (5 + NS) q doubles per cell of grow(box, 3) (PLM: 6 + NS); write
@@ -17,8 +18,8 @@ re-reads). For a region of valid edges (nx, ny, nz), NS species, compute-type si
            both (D|O) flux arrays
 * flux2:   per direction, read 2 NT r per face, the two corrected fluxes (NF r per face
            of their regions), NVAR doubles of u and one divu per face; write NVAR + 2
-           doubles per face of the box
-* consup:  read 3 (NVAR + 2) doubles per face, write NVAR doubles per cell
+           values per face of the box (FP32 in the mixed form without flux export)
+* consup:  read 3 (NVAR + 2) final-flux values per face, write NVAR doubles per cell
 
 The path-level figure is the survey's B_alg = 8 NVAR [(nx+8)(ny+8)(nz+8) + nx ny nz]
 bytes per box (read the grown state once, write the hydro source once).
@@ -54,8 +55,9 @@ def _faces(n, d, grow_other):
 def stage_bytes(stage, n, ns, r, ppm=True):
     """Algorithmic bytes of one launch of a hydro stage over one region of edges n."""
     nt, nf, nv, nq = 6 + ns, 7 + ns, 7 + ns, 8 + ns
+    ff = 4 if r == 4 else 8  # final-flux element size
     if stage == "ctoprim":
-        return _cells(n, 4) * 8 * (nv + nq + 6)
+        return _cells(n, 4) * 8 * (nv + nq + 6) + (_cells(n, 3) * nt * 4 if r == 4 else 0)
     if stage == "prep":
         nodes = (n[0] + 1) * (n[1] + 1) * (n[2] + 1)
         return _cells(n, 4) * 8 * (5 + ns) + _cells(n, 1) * 2 * r + nodes * 8
@@ -82,10 +84,10 @@ def stage_bytes(stage, n, ns, r, ppm=True):
         tot = 0
         for d in range(3):
             f = _faces(n, d, 0)
-            tot += f * (2 * nt * r + 2 * nf * r + nv * 8 + 8 + (nv + 2) * 8)
+            tot += f * (2 * nt * r + 2 * nf * r + nv * 8 + 8 + (nv + 2) * ff)
         return tot
     if stage == "consup":
-        return sum(_faces(n, d, 0) * (nv + 2) * 8 for d in range(3)) + n[0] * n[1] * n[2] * nv * 8
+        return sum(_faces(n, d, 0) * (nv + 2) * ff for d in range(3)) + n[0] * n[1] * n[2] * nv * 8
     raise ValueError(stage)
 
 

@@ -88,7 +88,7 @@ def test_fused_level_equals_per_box(prec):
     if prec == abi.PREC_FP64:
         np.testing.assert_array_equal(to_cpu(st_f.hsrc), to_cpu(st_b.hsrc))
     else:
-        # the FP32 pressure offset is the first cell's pressure of each region, so a
+        # the FP32 pressure offset is rho*R/W*T of each region's first cell, so a
         # fused level and its boxes agree to FP32 rounding of the offset only
         l1, linf = rel_err(to_cpu(st_f.hsrc), to_cpu(st_b.hsrc))
         assert l1 <= 1e-8 and linf <= 1e-7, (l1, linf)

@@ -34,7 +34,7 @@ constexpr int kMinBlocks[K_NSTAGE][3] = {
   {0, 4, 5},  // trace
   {0, 6, 8},  // flux0
   {0, 6, 8},  // flux1
-  {0, 4, 5},  // flux2
+  {4, 5, 6},  // flux2
   {0, 0, 0},  // consup
 };
 
@@ -69,6 +69,18 @@ __device__ __forceinline__ bool item_of(const pcg::StageArgs& a, Item& it) {
   return true;
 }
 
+// The segment of this block and the block's index within it (tiled stages).
+__device__ __forceinline__ const pcg::Seg& seg_of(const pcg::StageArgs& a, int64_t& local_block) {
+  const int64_t blk = blockIdx.x;
+  int lo = 0, hi = a.nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.segs[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
+  }
+  local_block = blk - a.segs[lo].blk0;
+  return a.segs[lo];
+}
+
 // A pointer positioned at one cell of a view: components n at p[n * ns].
 template <class T>
 struct CellPtr {
@@ -89,19 +101,19 @@ __device__ __forceinline__ int64_t dstride(const V4<T>& v, int d) {
   return d == 0 ? 1 : d == 1 ? v.js : v.ks;
 }
 
-// The pressure offset of a region for the FP32 arithmetic (see PDev): rho * rmix * T of
-// the region's first valid cell, from the conserved state and its stored temperature
-// (any constant of the region would do; this one needs no neighbour and no Newton
-// solve, so every stage computes the same value); zero for FP64.
+// The pressure offset of a region for the FP32 arithmetic (see PDev): the ideal-gas
+// pressure RU * sum(rhoY_k / W_k) * T of the region's first valid cell, from the
+// conserved partial densities and the stored temperature (any constant of the region
+// would do; this one needs no neighbour, no division and no Newton solve, so every
+// stage computes the same value cheaply); zero for FP64.
 template <int NS, bool MIX, class R>
 __device__ __forceinline__ double p0_of(const pcg::Region& rg) {
   if constexpr (PDev<R>::on) {
     const CellPtr<const double> u{&v4<const double>(rg.uin)(rg.lo[0], rg.lo[1], rg.lo[2], 0), rg.uin.ns};
-    const double rho = u[pcg::URHO];
-    double y[NS];
+    double w[NS];
 #pragma unroll
-    for (int n = 0; n < NS; ++n) y[n] = u[pcg::UFS + n] / rho;
-    return rho * Eos<NS, MIX, double>::rmix(y) * u[pcg::UTEMP];
+    for (int n = 0; n < NS; ++n) w[n] = u[pcg::UFS + n];
+    return Eos<NS, MIX, double>::rmix(w) * u[pcg::UTEMP];
   } else {
     return 0.0;
   }
@@ -652,28 +664,23 @@ __global__ void __launch_bounds__(128, MINB) k_flux1(pcg::StageArgs a) {
 // Source/Godunov.H:639-845 (pc_transdd) for one side: fx is the O1-flux corrected by
 // O2 positioned at the cell's low O1-face, fy the O2-flux corrected by O1 at the low
 // O2-face.
-template <int NS, bool EXACT, class R>
-__device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>& fx, int64_t xst,
-                                             const CellPtr<const R>& fy, int64_t yst, R cdtdx0, R cdtdx1, R hdt,
-                                             R c, bool has_src, const CellPtr<const double>& sq, R p0, R* out) {
+// pc_transdd (Source/Godunov.H:639-845) split in two. transdd_corr forms the part that
+// depends only on the cell the traced state belongs to: the two transverse flux
+// differences of each conserved component and the two transverse pressure updates,
+//   K[n]      = cdtdx0 (F^x_{+} - F^x)[n] + cdtdx1 (F^y_{+} - F^y)[n],  n < 5 + NS
+//   K[5 + NS] = cdtdx0 (dAup_x + pav_x dAu_x (c - 1)),  K[6 + NS] the same in y,
+// with c the cell's gamma_c (in the FP32 form both pressure updates also carry
+// p0 c dAu). transdd_apply then corrects one traced state with K. The two D-faces of
+// a cell share its K, so a thread computes it once for both. Every value is formed by
+// the reference's expressions in the reference's order.
+template <int NS> constexpr int ncorr() { return 7 + NS; }
+
+template <int NS, class R>
+__device__ __forceinline__ void transdd_corr(const CellPtr<const R>& fx, int64_t xst, const CellPtr<const R>& fy,
+                                             int64_t yst, R cdtdx0, R cdtdx1, R c, R p0, R* K) {
   const CellPtr<const R> gx = shift(fx, xst), gy = shift(fy, yst);
-#define FD(n) (cdtdx0 * (gx[n] - fx[n]) + cdtdx1 * (gy[n] - fy[n]))
-  const R flxrho = FD(0);
-  const R flxu = FD(1);
-  const R flxv = FD(2);
-  const R flxw = FD(3);
-  const R flxe = FD(4);
-  const R rr = qn[pcg::TR_RHO];
-  const R rrnew = rr - flxrho;
-  const R irrnew = EXACT ? R(0) : rrcp(rrnew);
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    const R srcpass = has_src ? R(sq[pcg::QFS + n]) : R(0);
-    const R compn = FD(pcg::FL_Y + n);
-    const R compo = rr * qn[pcg::TR_Y + n] - compn;
-    out[pcg::TR_Y + n] = (EXACT ? compo / rrnew : compo * irrnew) + hdt * srcpass;
-  }
-#undef FD
+  for (int n = 0; n < pcg::FL_Y + NS; ++n) K[n] = cdtdx0 * (gx[n] - fx[n]) + cdtdx1 * (gy[n] - fy[n]);
   const int gp = pcg::FL_Y + NS, gu = pcg::FL_Y + NS + 1;
   const R dAupx = gx[gp] * gx[gu] - fx[gp] * fx[gu];
   const R pavx = R(0.5) * (gx[gp] + fx[gp]);
@@ -687,8 +694,30 @@ __device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>
     dptx = dptx + p0 * c * dAux;
     dpty = dpty + p0 * c * dAuy;
   }
-  const R pxnew = cdtdx0 * dptx;
-  const R pynew = cdtdx1 * dpty;
+  K[5 + NS] = cdtdx0 * dptx;
+  K[6 + NS] = cdtdx1 * dpty;
+}
+
+template <int NS, bool EXACT, class R>
+__device__ __forceinline__ void transdd_apply(const R* qn, const R* K, R hdt, bool has_src,
+                                              const CellPtr<const double>& sq, R p0, R* out) {
+  const R flxrho = K[0];
+  const R flxu = K[1];
+  const R flxv = K[2];
+  const R flxw = K[3];
+  const R flxe = K[4];
+  const R rr = qn[pcg::TR_RHO];
+  const R rrnew = rr - flxrho;
+  const R irrnew = EXACT ? R(0) : rrcp(rrnew);
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    const R srcpass = has_src ? R(sq[pcg::QFS + n]) : R(0);
+    const R compn = K[pcg::FL_Y + n];
+    const R compo = rr * qn[pcg::TR_Y + n] - compn;
+    out[pcg::TR_Y + n] = (EXACT ? compo / rrnew : compo * irrnew) + hdt * srcpass;
+  }
+  const R pxnew = K[5 + NS];
+  const R pynew = K[6 + NS];
   const R s0 = has_src ? R(sq[pcg::QRHO]) : R(0), s1 = has_src ? R(sq[pcg::QU]) : R(0);
   const R s2 = has_src ? R(sq[pcg::QV]) : R(0), s3 = has_src ? R(sq[pcg::QW]) : R(0);
   const R s4 = has_src ? R(sq[pcg::QREINT]) : R(0), s5 = has_src ? R(sq[pcg::QPRES]) : R(0);
@@ -713,43 +742,68 @@ __device__ __forceinline__ void transdd_side(const R* qn, const CellPtr<const R>
   out[pcg::TR_P] = dmax(pn, pfloor(Lim<R>::tiny(), p0));
 }
 
-// Final fluxes (Source/Godunov.cpp:392-438) followed by the per-face flux adjustments
-// of pc_adjust_fluxes (Source/Hydro.cpp:380-413): pc_artif_visc (Godunov.H:1067-1138),
-// pc_norm_spec_flx and pc_ext_flx (Hydro.H:835-865), all in FP64.
-template <int NS, bool MIX, bool EXACT, int D, class R>
-__device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+// pc_artif_visc (Source/Godunov.H:1105-1132) with the coefficient visc = dx * difmag *
+// min(0, div u) already formed, then pc_norm_spec_flx (Source/Hydro.H:835-849), on the
+// fluxes of one d-face; T is the flux arithmetic type. The increments are formed as
+// visc * (u_i - u_{i-1}) in FP64, the reference's order of operations.
+template <int NS, int D, class T>
+__device__ __forceinline__ void adjust_fluxes(T* fl, const CellPtr<const double>& u, int64_t ud, double visc,
+                                              bool at_bndry) {
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); n++) {
+    if (n == pcg::UTEMP) continue;
+    const bool is_tang = (n == pcg::UMX || n == pcg::UMY || n == pcg::UMZ) && (n != pcg::UMX + D);
+    if (!(at_bndry && is_tang)) fl[n] += T(visc * (u[n] - u.p[-ud + (int64_t)n * u.ns]));
+  }
+  fl[pcg::UTEMP] = T(0);
+  T summ = T(0);
+#pragma unroll
+  for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) summ += fl[n];
+  const T fac = (summ != T(0)) ? fl[pcg::URHO] / summ : T(1);
+#pragma unroll
+  for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) fl[n] *= fac;
+}
+
+// The transverse correction of the cell (i, j, k) for the final D-fluxes: the
+// (O1|O2) and (O2|O1) fluxes on the cell's faces and the cell's gamma_c.
+template <int NS, int D, class R>
+__device__ __forceinline__ void flux2_corr(const pcg::Region& rg, int i, int j, int k, R cdtdx0, R cdtdx1, R p0,
+                                           R* K) {
   constexpr int O1 = (D == 0) ? 1 : 0;
   constexpr int O2 = (D == 2) ? 1 : 2;
-  const V4<const double> qav = v4<const double>(rg.qa);
-  const CellPtr<const double> qa = at(qav, i, j, k);
   const V4<const R> fxv = v4<const R>(rg.fdo[O1][O2]);
   const V4<const R> fyv = v4<const R>(rg.fdo[O2][O1]);
-  const CellPtr<const R> fx = at(fxv, i, j, k), fy = at(fyv, i, j, k);
-  const int64_t xd = dstride(fxv, D), yd = dstride(fyv, D);
-  const int64_t xst = dstride(fxv, O1), yst = dstride(fyv, O2);
-  const double dt = dt_of(a, rg);
-  const R cdtdx0 = R(0.5 * dt / rg.dx[O1]);
-  const R cdtdx1 = R(0.5 * dt / rg.dx[O2]);
-  const R hdt = R(0.5 * dt);
-  const double p0d = p0_of<NS, MIX, R>(rg);
-  const R p0 = R(p0d);
+  const R c = R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC));
+  transdd_corr<NS, R>(at(fxv, i, j, k), dstride(fxv, O1), at(fyv, i, j, k), dstride(fyv, O2), cdtdx0, cdtdx1, c, p0,
+                      K);
+}
+
+// One traced state of the D-face (i, j, k) after pc_transdd: SIDE 0 the left state
+// (trm, source terms of the cell behind the face), 1 the right state (trp).
+template <int NS, bool EXACT, int D, int SIDE, class R>
+__device__ __forceinline__ void flux2_state(const pcg::Region& rg, int i, int j, int k, const R* K, R hdt, R p0,
+                                            R* q) {
   const bool has_src = rg.srcq.p != nullptr;
   const V4<const double> sqv = v4<const double>(rg.srcq);
-  const CellPtr<const double> sqp = has_src ? at(sqv, i, j, k) : CellPtr<const double>{nullptr, 0};
-  const CellPtr<const double> sqm = has_src ? shift(sqp, -dstride(sqv, D)) : sqp;
-  R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
-  load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
-  transdd_side<NS, EXACT, R>(qn, shift(fx, -xd), xst, shift(fy, -yd), yst, cdtdx0, cdtdx1, hdt,
-                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), has_src, sqm, p0, ql);
-  load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qn);
-  transdd_side<NS, EXACT, R>(qn, fx, xst, fy, yst, cdtdx0, cdtdx1, hdt, R(qa[pcg::QGAMC]), has_src, sqp, p0, qr);
+  CellPtr<const double> sq = has_src ? at(sqv, i, j, k) : CellPtr<const double>{nullptr, 0};
+  if (SIDE == 0 && has_src) sq = shift(sq, -dstride(sqv, D));
+  R qn[pcg::nt_comps(NS)];
+  load_state<NS, R>(at(v4<R>(SIDE == 0 ? rg.trm[D] : rg.trp[D]), i, j, k), qn);
+  transdd_apply<NS, EXACT, R>(qn, K, hdt, has_src, sq, p0, q);
+}
+
+// Final fluxes (Source/Godunov.cpp:392-438) followed by the per-face flux adjustments
+// of pc_adjust_fluxes (Source/Hydro.cpp:380-413): pc_artif_visc (Godunov.H:1067-1138),
+// pc_norm_spec_flx and pc_ext_flx (Hydro.H:835-865). ql and qr are the face's traced
+// states after their transverse corrections.
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k,
+                                           const R* ql, const R* qr, double p0d) {
+  constexpr int O1 = (D == 0) ? 1 : 0;
+  constexpr int O2 = (D == 2) ? 1 : 2;
   R flr[pcg::nvar(NS)], gun, gpres;
   face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, flr, gun, gpres);
-  double fl[pcg::nvar(NS)];
-#pragma unroll
-  for (int n = 0; n < pcg::nvar(NS); ++n) fl[n] = (n == pcg::UTEMP) ? 0.0 : double(flr[n]);
-  if constexpr (PDev<R>::on) fl[pcg::UMX + D] += p0d;  // momentum flux back to the absolute pressure
-  // pc_artif_visc
+  // pc_artif_visc coefficient: difmag * min(0, average of the four nodal div u of the face)
   const V4<const double> dv = v4<const double>(rg.divu);
   const int ji = i + (O1 == 0), jj = j + (O1 == 1), jk = k + (O1 == 2);
   const int ki = i + (O2 == 0), kj = j + (O2 == 1), kk = k + (O2 == 2);
@@ -759,38 +813,35 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
   const bool at_bndry = (idx == rg.domlo[D] && rg.bclo[D] == pcg::BC_NO_SLIP_WALL) ||
                         (idx == rg.domhi[D] + 1 && rg.bchi[D] == pcg::BC_NO_SLIP_WALL);
-  const double dxd = rg.dx[D];
+  const double visc = rg.dx[D] * div;
   const V4<const double> uv = v4<const double>(rg.uin);
   const CellPtr<const double> u = at(uv, i, j, k);
   const int64_t ud = dstride(uv, D);
-#pragma unroll
-  for (int n = 0; n < pcg::nvar(NS); n++) {
-    if (n == pcg::UTEMP) continue;
-    const bool is_tang = (n == pcg::UMX || n == pcg::UMY || n == pcg::UMZ) && (n != pcg::UMX + D);
-    if (!(at_bndry && is_tang)) fl[n] += dxd * div * (u[n] - u.p[-ud + (int64_t)n * u.ns]);
-  }
-  fl[pcg::UTEMP] = 0.0;
-  // pc_norm_spec_flx
-  double summ = 0.0;
-#pragma unroll
-  for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) summ += fl[n];
-  const double fac = (summ != 0.0) ? fl[pcg::URHO] / summ : 1.0;
-#pragma unroll
-  for (int n = pcg::UFS; n < pcg::UFS + NS; ++n) fl[n] *= fac;
-  // pc_ext_flx
   const double ar = rg.area[D].p ? v4<const double>(rg.area[D])(i, j, k) : rg.area_u[D];
-  if (PDev<R>::on && rg.ff_single) {
-    // FP32 final fluxes for the FP64 divergence accumulation, normal momentum flux and
-    // Godunov pressure as deviations from p0 (the divergence is shift invariant)
-    fl[pcg::UMX + D] -= p0d;
-    const CellPtr<float> ff = at(v4<float>(rg.ff[D]), i, j, k);
+  if constexpr (PDev<R>::on) {
+    if (rg.ff_single) {
+      // FP32 final fluxes for the FP64 divergence accumulation: the adjustments run in
+      // FP32 on the FP32 Riemann fluxes (each viscous increment is formed in FP64 from the
+      // FP64 state and rounded once); the normal momentum flux and the Godunov pressure
+      // stay deviations from p0, which cancel in the divergence
+      flr[pcg::UTEMP] = 0.f;
+      adjust_fluxes<NS, D, float>(flr, u, ud, visc, at_bndry);
+      const float arf = float(ar);
+      const CellPtr<float> ff = at(v4<float>(rg.ff[D]), i, j, k);
 #pragma unroll
-    for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = float(fl[n] * ar);
-    const CellPtr<float> qe = at(v4<float>(rg.qec[D]), i, j, k);
-    qe[0] = float(gpres);
-    qe[1] = float(gun);
-    return;
+      for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = flr[n] * arf;
+      const CellPtr<float> qe = at(v4<float>(rg.qec[D]), i, j, k);
+      qe[0] = float(gpres);
+      qe[1] = float(gun);
+      return;
+    }
   }
+  double fl[pcg::nvar(NS)];
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) fl[n] = (n == pcg::UTEMP) ? 0.0 : double(flr[n]);
+  if constexpr (PDev<R>::on) fl[pcg::UMX + D] += p0d;  // momentum flux back to the absolute pressure
+  adjust_fluxes<NS, D, double>(fl, u, ud, visc, at_bndry);
+  // pc_ext_flx
   const CellPtr<double> ff = at(v4<double>(rg.ff[D]), i, j, k);
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = fl[n] * ar;
@@ -799,14 +850,113 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   qe[1] = double(gun);
 }
 
+// One launch covers the final fluxes of all three directions. The two D-faces of a cell
+// share its transverse correction, so each thread computes one correction per face:
+//  * x-faces: a warp covers 32 consecutive cells of one (j, k) row and solves the 31
+//    faces between them; each lane takes its right neighbour's correction by shuffle;
+//  * y- and z-faces: a warp covers 32 consecutive i of one row and each thread marches
+//    pcg::F2_MARCH faces along D, carrying the correction of the cell behind the face.
+// A block is four such warps (four rows). The per-segment tile counts are computed by
+// flux2_tiles on the host.
+template <int NS, bool MIX, bool EXACT, class R>
+__device__ __forceinline__ void flux2_consts(const pcg::StageArgs& a, const pcg::Region& rg, int D, R& cdtdx0,
+                                             R& cdtdx1, R& hdt, double& p0d) {
+  const int O1 = (D == 0) ? 1 : 0;
+  const int O2 = (D == 2) ? 1 : 2;
+  const double dt = dt_of(a, rg);
+  cdtdx0 = R(0.5 * dt / rg.dx[O1]);
+  cdtdx1 = R(0.5 * dt / rg.dx[O2]);
+  hdt = R(0.5 * dt);
+  p0d = p0_of<NS, MIX, R>(rg);
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t) {
+  const pcg::Region& rg = a.regions[sg.region];
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  const int64_t nti = (sg.n[0] + 30) / 31, nr = (sg.n[1] + 3) / 4;
+  const int ti = (int)(t % nti);
+  const int64_t rest = t / nti;
+  const int j = sg.lo[1] + (int)(rest % nr) * 4 + row;
+  const int k = sg.lo[2] + (int)(rest / nr);
+  if (j >= sg.lo[1] + sg.n[1]) return;  // whole warp
+  const int ic = sg.lo[0] - 1 + ti * 31 + lane;  // this lane's cell; faces ic + 1 ...
+  const int ilast = sg.lo[0] + sg.n[0] - 1;      // last face (= last cell needed)
+  R cdtdx0, cdtdx1, hdt;
+  double p0d;
+  flux2_consts<NS, MIX, EXACT, R>(a, rg, 0, cdtdx0, cdtdx1, hdt, p0d);
+  R K[ncorr<NS>()], Kr[ncorr<NS>()];
+  if (ic <= ilast) {
+    flux2_corr<NS, 0, R>(rg, ic, j, k, cdtdx0, cdtdx1, R(p0d), K);
+  } else {
+#pragma unroll
+    for (int n = 0; n < ncorr<NS>(); ++n) K[n] = R(0);
+  }
+#pragma unroll
+  for (int n = 0; n < ncorr<NS>(); ++n) Kr[n] = __shfl_down_sync(0xffffffffu, K[n], 1);
+  const int i = ic + 1;  // face between this lane's cell and the next lane's
+  if (lane == 31 || i > ilast) return;
+  R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+  flux2_state<NS, EXACT, 0, 0, R>(rg, i, j, k, K, hdt, R(p0d), ql);
+  flux2_state<NS, EXACT, 0, 1, R>(rg, i, j, k, Kr, hdt, R(p0d), qr);
+  flux2_face<NS, MIX, EXACT, 0, R>(a, rg, i, j, k, ql, qr, p0d);
+}
+
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kcarry) {
+  const pcg::Region& rg = a.regions[sg.region];
+  constexpr int RA = (D == 1) ? 2 : 1;  // row axis; lanes run along i, the march along D
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  const int64_t nti = (sg.n[0] + 31) / 32, nr = (sg.n[RA] + 3) / 4;
+  const int ti = (int)(t % nti);
+  const int64_t rest = t / nti;
+  const int r = sg.lo[RA] + (int)(rest % nr) * 4 + row;
+  const int m0 = sg.lo[D] + (int)(rest / nr) * pcg::F2_MARCH;
+  const int i = sg.lo[0] + ti * 32 + lane;
+  if (i >= sg.lo[0] + sg.n[0] || r >= sg.lo[RA] + sg.n[RA]) return;
+  const int m1 = min(m0 + pcg::F2_MARCH, sg.lo[D] + sg.n[D]);
+  R cdtdx0, cdtdx1, hdt;
+  double p0d;
+  flux2_consts<NS, MIX, EXACT, R>(a, rg, D, cdtdx0, cdtdx1, hdt, p0d);
+  const R p0 = R(p0d);
+  // the correction of the cell behind the face waits in one of this thread's two
+  // shared-memory slots (component-major, conflict free): each step first forms the
+  // correction of the next cell with nothing else live, then corrects both states
+  R* sl = kcarry + threadIdx.x;
+  R* sr = kcarry + ncorr<NS>() * 128 + threadIdx.x;
+  R K[ncorr<NS>()];
+  if (D == 1)
+    flux2_corr<NS, D, R>(rg, i, m0 - 1, r, cdtdx0, cdtdx1, p0, K);
+  else
+    flux2_corr<NS, D, R>(rg, i, r, m0 - 1, cdtdx0, cdtdx1, p0, K);
+#pragma unroll
+  for (int n = 0; n < ncorr<NS>(); ++n) sl[n * 128] = K[n];
+  for (int m = m0; m < m1; ++m) {
+    const int j = (D == 1) ? m : r, k = (D == 1) ? r : m;
+    flux2_corr<NS, D, R>(rg, i, j, k, cdtdx0, cdtdx1, p0, K);
+#pragma unroll
+    for (int n = 0; n < ncorr<NS>(); ++n) sr[n * 128] = K[n];
+    R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+    flux2_state<NS, EXACT, D, 1, R>(rg, i, j, k, K, hdt, p0, qr);
+#pragma unroll
+    for (int n = 0; n < ncorr<NS>(); ++n) K[n] = sl[n * 128];
+    flux2_state<NS, EXACT, D, 0, R>(rg, i, j, k, K, hdt, p0, ql);
+    R* tmp = sl;
+    sl = sr;
+    sr = tmp;
+    flux2_face<NS, MIX, EXACT, D, R>(a, rg, i, j, k, ql, qr, p0d);
+  }
+}
+
 template <int NS, bool MIX, bool EXACT, class R, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
-  Item it;
-  if (!item_of(a, it)) return;
-  switch (it.variant) {
-    case 0: flux2_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
-    case 1: flux2_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
-    default: flux2_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  __shared__ R kcarry[2 * ncorr<NS>() * 128];
+  int64_t t;
+  const pcg::Seg& sg = seg_of(a, t);
+  switch (sg.variant) {
+    case 0: flux2_x<NS, MIX, EXACT, R>(a, sg, t); break;
+    case 1: flux2_march<NS, MIX, EXACT, 1, R>(a, sg, t, kcarry); break;
+    default: flux2_march<NS, MIX, EXACT, 2, R>(a, sg, t, kcarry); break;
   }
 }
 

@@ -101,6 +101,15 @@ struct Region {
 // A run of thread blocks of one stage working on one region (and one variant, e.g.
 // a direction or a (direction, other direction) pair) over the index box
 // [lo, lo + n).
+// Final-flux stage tiling (k_flux2): x-faces take 31 faces per 32-lane warp, y- and
+// z-faces march F2_MARCH faces per thread along their direction; four rows per block.
+constexpr int F2_MARCH = 4;
+PCG_HD constexpr int64_t flux2_tiles(int d, const int32_t n[3]) {
+  return d == 0 ? int64_t((n[0] + 30) / 31) * ((n[1] + 3) / 4) * n[2]
+       : d == 1 ? int64_t((n[0] + 31) / 32) * ((n[2] + 3) / 4) * ((n[1] + F2_MARCH - 1) / F2_MARCH)
+                : int64_t((n[0] + 31) / 32) * ((n[1] + 3) / 4) * ((n[2] + F2_MARCH - 1) / F2_MARCH);
+}
+
 struct Seg {
   int32_t region;
   int32_t variant;

@@ -81,3 +81,62 @@ class LevelStepper:
     def close(self):
         self.graph = None
         self.plan.close()
+
+
+class HostPipeline:
+    """Advance host-resident level states through the device, one level step each.
+
+    Every submitted state goes host -> device (pinned memory), takes one graph-captured
+    level step and comes back device -> host. ``depth`` device slots (a LevelStepper each)
+    rotate so that the upload of submission k+1, the step of submission k and the download
+    of submission k-1 run at the same time: uploads and downloads use separate copy
+    streams (the two DMA directions are independent) and the steps share one compute
+    stream. Per submission the full state crosses the bus once each way.
+    """
+
+    def __init__(self, level, depth=2, **stepper_kw):
+        import torch
+
+        self.torch = torch
+        self.slots = [LevelStepper(level, **stepper_kw) for _ in range(depth)]
+        for s in self.slots:
+            s.capture()
+        dev = self.slots[0].dev
+        self.up, self.comp, self.down = (torch.cuda.Stream(device=dev) for _ in range(3))
+        ev = lambda: [torch.cuda.Event() for _ in range(depth)]  # noqa: E731
+        self.ev_in, self.ev_step, self.ev_out = ev(), ev(), ev()
+        self.used = [False] * depth
+        self.k = 0
+        self.ncells = self.slots[0].ncells
+        self.state_bytes = self.slots[0].state.data.numel() * 8
+
+    def submit(self, host_in, host_out):
+        """Enqueue one advance of ``host_in`` (pinned, the level's state shape) into
+        ``host_out`` (pinned; must not be read before :meth:`synchronize`)."""
+        torch = self.torch
+        b = self.k % len(self.slots)
+        slot = self.slots[b]
+        if self.used[b]:
+            self.up.wait_event(self.ev_out[b])  # the slot's previous result has left the device
+        with torch.cuda.stream(self.up):
+            slot.state.data.copy_(host_in, non_blocking=True)
+            self.ev_in[b].record(self.up)
+        self.comp.wait_event(self.ev_in[b])
+        with torch.cuda.stream(self.comp):
+            slot.replay()
+            self.ev_step[b].record(self.comp)
+        self.down.wait_event(self.ev_step[b])
+        with torch.cuda.stream(self.down):
+            host_out.copy_(slot.state.data, non_blocking=True)
+            self.ev_out[b].record(self.down)
+        self.used[b] = True
+        self.k += 1
+
+    def synchronize(self):
+        for s in (self.up, self.comp, self.down):
+            s.synchronize()
+
+    def close(self):
+        self.synchronize()
+        for s in self.slots:
+            s.close()

@@ -48,9 +48,9 @@ thread_local std::string g_err;
 // level; pcg_set_launch_variant (the autotuner) overrides them.
 std::mutex g_var_mu;
 int g_variant[3][2][7] = {
-  {{0, 0, 2, 0, 2, 0, 0}, {2, 0, 1, 1, 1, 0, 0}},  // FP64 reference order
-  {{2, 0, 1, 0, 0, 1, 0}, {2, 0, 1, 0, 0, 1, 0}},  // FP64 with FMA
-  {{0, 0, 2, 0, 2, 0, 0}, {2, 0, 2, 1, 1, 1, 0}},  // mixed
+  {{0, 0, 2, 0, 2, 2, 0}, {2, 0, 1, 1, 2, 0, 0}},  // FP64 reference order
+  {{2, 0, 1, 0, 0, 0, 0}, {2, 0, 1, 0, 0, 0, 0}},  // FP64 with FMA
+  {{0, 0, 2, 0, 2, 0, 0}, {2, 0, 2, 2, 2, 1, 0}},  // mixed
 };
 int variant_of(int prec, int ns, int stage) {
   std::lock_guard<std::mutex> lk(g_var_mu);
@@ -226,7 +226,8 @@ void add_seg(Layout& L, int stage, int region, int variant, const IBox& b) {
   s.count = b.cells();
   s.blk0 = L.nblocks[stage];
   L.segs[stage].push_back(s);
-  L.nblocks[stage] += (stage == K_FLUX2) ? pcg::flux2_tiles(variant, s.n) : (s.count + kThreads - 1) / kThreads;
+  const bool tiled = stage == K_FLUX2 || (stage == K_FLUX1 && pcg::flux1_shared(L.esz));
+  L.nblocks[stage] += tiled ? pcg::face_tiles(variant, s.n) : (s.count + kThreads - 1) / kThreads;
 }
 
 void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool single) {

@@ -33,7 +33,7 @@ constexpr int kMinBlocks[K_NSTAGE][3] = {
   {0, 0, 0},  // prep
   {0, 4, 5},  // trace
   {0, 6, 8},  // flux0
-  {0, 6, 8},  // flux1
+  {4, 5, 6},  // flux1
   {4, 5, 6},  // flux2
   {0, 0, 0},  // consup
 };
@@ -568,33 +568,78 @@ __global__ void __launch_bounds__(128, MINB) k_flux0(pcg::StageArgs a) {
   }
 }
 
-// Source/Godunov.H:455-633 (pc_transdo) for one side: qn is the traced state, f the
-// O-flux positioned at the cell's low O-face (its high O-face is at +ostride).
-template <int NS, bool EXACT, class R>
-__device__ __forceinline__ void transdo_side(const R* qn, const CellPtr<const R>& f, int64_t ostride, R cdtdx, R c,
-                                             R p0, R* out) {
-  const CellPtr<const R> g = shift(f, ostride);
-  const R flxrho = cdtdx * (g[0] - f[0]);
-  const R flxu = cdtdx * (g[1] - f[1]);
-  const R flxv = cdtdx * (g[2] - f[2]);
-  const R flxw = cdtdx * (g[3] - f[3]);
-  const R flxe = cdtdx * (g[4] - f[4]);
+// The march of one thread of a y- or z-face stage (k_flux1, k_flux2): threads in linear
+// order over i (fastest), the row axis and the chunks of pcg::FACE_MARCH faces along D.
+template <int D>
+__device__ __forceinline__ bool march_of(const pcg::Seg& sg, int64_t t, int& i, int& r, int& m0, int& m1) {
+  constexpr int RA = (D == 1) ? 2 : 1;
+  const int64_t local = t * blockDim.x + threadIdx.x;
+  if (local >= pcg::face_threads(D, sg.n)) return false;
+  const int64_t q = local / sg.n[0];
+  i = sg.lo[0] + (int)(local - q * sg.n[0]);
+  r = sg.lo[RA] + (int)(q % sg.n[RA]);
+  m0 = sg.lo[D] + (int)(q / sg.n[RA]) * pcg::FACE_MARCH;
+  m1 = min(m0 + pcg::FACE_MARCH, sg.lo[D] + sg.n[D]);
+  return true;
+}
+
+// pc_transdo (Source/Godunov.H:455-633) split like pc_transdd below: transdo_corr forms
+// the part that depends only on the cell the traced state belongs to, the O-flux
+// differences of the conserved components and the pressure update,
+//   K[n]      = cdtdx (F^O_{+} - F^O)[n],  n < 5 + NS,
+//   K[5 + NS] = cdtdx (dAup + pav dAu (c - 1))   (+ p0 c dAu in the FP32 form),
+// and transdo_apply corrects one traced state with it, by the reference's expressions.
+template <int NS> constexpr int ncorr1() { return 6 + NS; }
+
+// The O-correction of one cell formed on demand from its two O-fluxes (component n of K).
+template <int NS, class R>
+struct TransdoCorr {
+  CellPtr<const R> f, g;
+  R cdtdx, c, p0;
+  __device__ __forceinline__ R operator()(int n) const {
+    if (n < pcg::FL_Y + NS) return cdtdx * (g[n] - f[n]);
+    const R pggp = g[pcg::FL_Y + NS];
+    const R pggm = f[pcg::FL_Y + NS];
+    const R ugp = g[pcg::FL_Y + NS + 1];
+    const R ugm = f[pcg::FL_Y + NS + 1];
+    const R dAup = pggp * ugp - pggm * ugm;
+    const R pav = R(0.5) * (pggp + pggm);
+    const R dAu = ugp - ugm;
+    R dpt = dAup + pav * dAu * (c - R(1));
+    if constexpr (PDev<R>::on) dpt = dpt + p0 * c * dAu;
+    return cdtdx * dpt;
+  }
+};
+// A correction already formed (K[n]).
+template <class R>
+struct CorrArray {
+  const R* K;
+  __device__ __forceinline__ R operator()(int n) const { return K[n]; }
+};
+
+template <int NS, class R>
+__device__ __forceinline__ void transdo_corr(const CellPtr<const R>& f, int64_t ostride, R cdtdx, R c, R p0, R* K) {
+  const TransdoCorr<NS, R> kc{f, shift(f, ostride), cdtdx, c, p0};
+#pragma unroll
+  for (int n = 0; n < ncorr1<NS>(); ++n) K[n] = kc(n);
+}
+
+template <int NS, bool EXACT, class R, class KF>
+__device__ __forceinline__ void transdo_apply(const R* qn, const KF& K, R p0, R* out) {
+  const R flxrho = K(0);
+  const R flxu = K(1);
+  const R flxv = K(2);
+  const R flxw = K(3);
+  const R flxe = K(4);
   const R rr = qn[pcg::TR_RHO];
   const R rrnew = rr - flxrho;
   const R irrnew = EXACT ? R(0) : rrcp(rrnew);
 #pragma unroll
   for (int n = 0; n < NS; n++) {
-    const R compn = cdtdx * (g[pcg::FL_Y + n] - f[pcg::FL_Y + n]);
+    const R compn = K(pcg::FL_Y + n);
     const R compo = rr * qn[pcg::TR_Y + n] - compn;
     out[pcg::TR_Y + n] = EXACT ? compo / rrnew : compo * irrnew;
   }
-  const R pggp = g[pcg::FL_Y + NS];
-  const R pggm = f[pcg::FL_Y + NS];
-  const R ugp = g[pcg::FL_Y + NS + 1];
-  const R ugm = f[pcg::FL_Y + NS + 1];
-  const R dAup = pggp * ugp - pggm * ugm;
-  const R pav = R(0.5) * (pggp + pggm);
-  const R dAu = ugp - ugm;
   R ru = qn[pcg::TR_U], rv = qn[pcg::TR_V], rw = qn[pcg::TR_W];
   const R ekin = R(0.5) * rr * (ru * ru + rv * rv + rw * rw);
   ru *= rr;
@@ -612,52 +657,203 @@ __device__ __forceinline__ void transdo_side(const R* qn, const CellPtr<const R>
   const R ke2 = runew * runew + rvnew * rvnew + rwnew * rwnew;
   const R rhoekin = EXACT ? R(0.5) * ke2 / rrnew : R(0.5) * ke2 * irrnew;
   out[pcg::TR_RE] = renew - rhoekin;
-  R dpt = dAup + pav * dAu * (c - R(1));
-  if constexpr (PDev<R>::on) dpt = dpt + p0 * c * dAu;
-  const R pnew = qn[pcg::TR_P] - cdtdx * dpt;
+  const R pnew = qn[pcg::TR_P] - K(5 + NS);
   out[pcg::TR_P] = dmax(pnew, pfloor(Lim<R>::very_small(), p0));
 }
 
-// Transverse predictor + paired Riemann solve for the pair (D|O) at D-face (i,j,k)
-// (Source/Godunov.cpp:246-384).
-template <int NS, bool MIX, bool EXACT, int D, int O, class R>
-__device__ __forceinline__ void flux1_pair(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
-  const V4<const double> qav = v4<const double>(rg.qa);
+// The O-correction of the cell (i, j, k): the first O-fluxes on its two O-faces and
+// its gamma_c.
+template <int NS, int O, class R>
+__device__ __forceinline__ void flux1_corr(const pcg::Region& rg, int i, int j, int k, R cdt, R p0, R* K) {
   const V4<const R> fov = v4<const R>(rg.fi[O]);
-  const int64_t dst_f = dstride(fov, D), ost_f = dstride(fov, O);
-  const CellPtr<const R> fo = at(fov, i, j, k);
-  const CellPtr<const double> qa = at(qav, i, j, k);
-  const R cdt = R(1.0 / 3.0 * dt_of(a, rg) / rg.dx[O]);
-  const R p0 = R(p0_of<NS, MIX, R>(rg));
-  R qn[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
-  load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), qn);
-  transdo_side<NS, EXACT, R>(qn, shift(fo, -dst_f), ost_f, cdt,
-                             R(qa.p[-dstride(qav, D) + (int64_t)pcg::QGAMC * qa.ns]), p0, ql);
-  load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qn);
-  transdo_side<NS, EXACT, R>(qn, fo, ost_f, cdt, R(qa[pcg::QGAMC]), p0, qr);
+  const R c = R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC));
+  transdo_corr<NS, R>(at(fov, i, j, k), dstride(fov, O), cdt, c, p0, K);
+}
+
+// The (D|O) flux at the D-face (i, j, k) from the left and right O-corrections
+// (Source/Godunov.cpp:246-384).
+template <int NS, bool EXACT, int D, int SIDE, class R, class KF>
+__device__ __forceinline__ void flux1_state_fn(const pcg::Region& rg, int i, int j, int k, const KF& K, R p0, R* q) {
+  R qn[pcg::nt_comps(NS)];
+  load_state<NS, R>(at(v4<R>(SIDE == 0 ? rg.trm[D] : rg.trp[D]), i, j, k), qn);
+  transdo_apply<NS, EXACT, R>(qn, K, p0, q);
+}
+template <int NS, bool EXACT, int D, int SIDE, class R>
+__device__ __forceinline__ void flux1_state(const pcg::Region& rg, int i, int j, int k, const R* K, R p0, R* q) {
+  flux1_state_fn<NS, EXACT, D, SIDE, R>(rg, i, j, k, CorrArray<R>{K}, p0, q);
+}
+
+// The O-correction of the cell (i, j, k), formed on demand.
+template <int NS, int O, class R>
+__device__ __forceinline__ TransdoCorr<NS, R> flux1_corr_fn(const pcg::Region& rg, int i, int j, int k, R cdt, R p0) {
+  const V4<const R> fov = v4<const R>(rg.fi[O]);
+  const CellPtr<const R> f = at(fov, i, j, k);
+  return TransdoCorr<NS, R>{f, shift(f, dstride(fov, O)), cdt, R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC)), p0};
+}
+
+template <int NS, bool MIX, bool EXACT, int D, int O, class R>
+__device__ __forceinline__ void flux1_riemann(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr) {
   R fl[pcg::nvar(NS)], gun, gpres;
   face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, fl, gun, gpres);
   store_tflux<NS, R>(at(v4<R>(rg.fdo[D][O]), i, j, k), fl, gun, gpres);
 }
 
+template <int NS, bool MIX, bool EXACT, int D, int O, class R>
+__device__ __forceinline__ void flux1_solve(const pcg::Region& rg, int i, int j, int k, const R* Kl, const R* Kr,
+                                            R p0) {
+  R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+  flux1_state<NS, EXACT, D, 0, R>(rg, i, j, k, Kl, p0, ql);
+  flux1_state<NS, EXACT, D, 1, R>(rg, i, j, k, Kr, p0, qr);
+  flux1_riemann<NS, MIX, EXACT, D, O, R>(rg, i, j, k, ql, qr);
+}
+
+template <int NS, class R>
+__device__ __forceinline__ R flux1_cdt(const pcg::StageArgs& a, const pcg::Region& rg, int O) {
+  return R(1.0 / 3.0 * dt_of(a, rg) / rg.dx[O]);
+}
+
+// x-faces, one face per thread in linear order (i fastest): each lane forms the
+// correction of the cell left of its face and reads the one right of it from the next
+// lane's shared-memory slot, which holds that cell whenever it is in the same row; the
+// last lane of a warp and the last face of a row form it themselves. The (0|O) flux
+// exists where the face's O index lies in the box.
+template <int NS, bool MIX, bool EXACT, int O, class R>
+__device__ __forceinline__ void flux1_x_pair(const pcg::StageArgs& a, const pcg::Region& rg, bool active, bool own_right,
+                                             int i, int j, int k, R p0, R* kx) {
+  const int c[3] = {i, j, k};
+  const bool has = active && c[O] >= rg.lo[O] && c[O] <= rg.hi[O];
+  const R cdt = flux1_cdt<NS, R>(a, rg, O);
+  R* mine = kx + threadIdx.x;
+  R K[ncorr1<NS>()];
+  if (has) {
+    flux1_corr<NS, O, R>(rg, i - 1, j, k, cdt, p0, K);
+#pragma unroll
+    for (int n = 0; n < ncorr1<NS>(); ++n) mine[n * 128] = K[n];
+  }
+  __syncwarp();
+  if (!has) return;
+  R Kr[ncorr1<NS>()];
+  if (own_right) {
+    flux1_corr<NS, O, R>(rg, i, j, k, cdt, p0, Kr);
+  } else {
+#pragma unroll
+    for (int n = 0; n < ncorr1<NS>(); ++n) Kr[n] = mine[n * 128 + 1];
+  }
+  flux1_solve<NS, MIX, EXACT, 0, O, R>(rg, i, j, k, K, Kr, p0);
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__device__ __forceinline__ void flux1_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kx) {
+  const pcg::Region& rg = a.regions[sg.region];
+  const int64_t local = t * blockDim.x + threadIdx.x;
+  const bool active = local < sg.count;
+  const int64_t q = local / sg.n[0];
+  const int i = sg.lo[0] + (int)(local - q * sg.n[0]);
+  const int j = sg.lo[1] + (int)(q % sg.n[1]);
+  const int k = sg.lo[2] + (int)(q / sg.n[1]);
+  const bool own_right = (threadIdx.x & 31) == 31 || i == sg.lo[0] + sg.n[0] - 1;
+  const R p0 = R(p0_of<NS, MIX, R>(rg));
+  flux1_x_pair<NS, MIX, EXACT, 1, R>(a, rg, active, own_right, i, j, k, p0, kx);
+  flux1_x_pair<NS, MIX, EXACT, 2, R>(a, rg, active, own_right, i, j, k, p0, kx + ncorr1<NS>() * 128);
+}
+
+// y- and z-faces: each thread marches pcg::FACE_MARCH faces along D (threads in linear
+// order over i, the row axis and the march chunks). Per partner O the correction of
+// the cell behind the face waits in the thread's shared-memory slot (component-major).
+template <int NS, bool MIX, bool EXACT, int D, int O, class R>
+__device__ __forceinline__ void flux1_march_pair(const pcg::Region& rg, int i, int r, int m, R cdt, R p0, R* slot) {
+  const int j = (D == 1) ? m : r, k = (D == 1) ? r : m;
+  R K[ncorr1<NS>()], qr[pcg::nt_comps(NS)], ql[pcg::nt_comps(NS)];
+  flux1_corr<NS, O, R>(rg, i, j, k, cdt, p0, K);
+  flux1_state<NS, EXACT, D, 1, R>(rg, i, j, k, K, p0, qr);
+#pragma unroll
+  for (int n = 0; n < ncorr1<NS>(); ++n) {
+    const R kl = slot[n * 128];
+    slot[n * 128] = K[n];
+    K[n] = kl;
+  }
+  flux1_state<NS, EXACT, D, 0, R>(rg, i, j, k, K, p0, ql);
+  flux1_riemann<NS, MIX, EXACT, D, O, R>(rg, i, j, k, ql, qr);
+}
+
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void flux1_march(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kcarry) {
+  const pcg::Region& rg = a.regions[sg.region];
+  constexpr int RA = (D == 1) ? 2 : 1;  // row axis, also the second partner
+  int i, r, m0, m1;
+  if (!march_of<D>(sg, t, i, r, m0, m1)) return;
+  const R p0 = R(p0_of<NS, MIX, R>(rg));
+  const bool has0 = i >= rg.lo[0] && i <= rg.hi[0];     // (D|0) exists
+  const bool hasr = r >= rg.lo[RA] && r <= rg.hi[RA];  // (D|RA) exists
+  const R cdt0 = flux1_cdt<NS, R>(a, rg, 0), cdtr = flux1_cdt<NS, R>(a, rg, RA);
+  R* s0 = kcarry + threadIdx.x;
+  R* sr = kcarry + ncorr1<NS>() * 128 + threadIdx.x;
+  R K[ncorr1<NS>()];
+  const int jb = (D == 1) ? m0 - 1 : r, kb = (D == 1) ? r : m0 - 1;
+  if (has0) {
+    flux1_corr<NS, 0, R>(rg, i, jb, kb, cdt0, p0, K);
+#pragma unroll
+    for (int n = 0; n < ncorr1<NS>(); ++n) s0[n * 128] = K[n];
+  }
+  if (hasr) {
+    flux1_corr<NS, RA, R>(rg, i, jb, kb, cdtr, p0, K);
+#pragma unroll
+    for (int n = 0; n < ncorr1<NS>(); ++n) sr[n * 128] = K[n];
+  }
+  for (int m = m0; m < m1; ++m) {
+    if (has0) flux1_march_pair<NS, MIX, EXACT, D, 0, R>(rg, i, r, m, cdt0, p0, s0);
+    if (hasr) flux1_march_pair<NS, MIX, EXACT, D, RA, R>(rg, i, r, m, cdtr, p0, sr);
+  }
+}
+
+// FP64 forms: one D-face per thread, both corrections of each pair formed by the
+// thread component by component as the state update consumes them (in FP64 the
+// shared forms above hold more registers than they save).
 template <int NS, bool MIX, bool EXACT, int D, class R>
 __device__ __forceinline__ void flux1_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
   constexpr int O1 = (D == 0) ? 1 : 0;
   constexpr int O2 = (D == 2) ? 1 : 2;
   const int c[3] = {i, j, k};
-  // fdo[D][O] covers O in the box and the third direction grown by one
-  if (c[O1] >= rg.lo[O1] && c[O1] <= rg.hi[O1]) flux1_pair<NS, MIX, EXACT, D, O1, R>(a, rg, i, j, k);
-  if (c[O2] >= rg.lo[O2] && c[O2] <= rg.hi[O2]) flux1_pair<NS, MIX, EXACT, D, O2, R>(a, rg, i, j, k);
+  const int di = (D == 0), dj = (D == 1), dk = (D == 2);
+  const R p0 = R(p0_of<NS, MIX, R>(rg));
+  // (D|O) exists where the face's O index lies in the box
+  if (c[O1] >= rg.lo[O1] && c[O1] <= rg.hi[O1]) {
+    const R cdt = flux1_cdt<NS, R>(a, rg, O1);
+    R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+    flux1_state_fn<NS, EXACT, D, 0, R>(rg, i, j, k, flux1_corr_fn<NS, O1, R>(rg, i - di, j - dj, k - dk, cdt, p0), p0,
+                                    ql);
+    flux1_state_fn<NS, EXACT, D, 1, R>(rg, i, j, k, flux1_corr_fn<NS, O1, R>(rg, i, j, k, cdt, p0), p0, qr);
+    flux1_riemann<NS, MIX, EXACT, D, O1, R>(rg, i, j, k, ql, qr);
+  }
+  if (c[O2] >= rg.lo[O2] && c[O2] <= rg.hi[O2]) {
+    const R cdt = flux1_cdt<NS, R>(a, rg, O2);
+    R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+    flux1_state_fn<NS, EXACT, D, 0, R>(rg, i, j, k, flux1_corr_fn<NS, O2, R>(rg, i - di, j - dj, k - dk, cdt, p0), p0,
+                                    ql);
+    flux1_state_fn<NS, EXACT, D, 1, R>(rg, i, j, k, flux1_corr_fn<NS, O2, R>(rg, i, j, k, cdt, p0), p0, qr);
+    flux1_riemann<NS, MIX, EXACT, D, O2, R>(rg, i, j, k, ql, qr);
+  }
 }
 
 template <int NS, bool MIX, bool EXACT, class R, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux1(pcg::StageArgs a) {
-  Item it;
-  if (!item_of(a, it)) return;
-  switch (it.variant) {
-    case 0: flux1_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
-    case 1: flux1_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
-    default: flux1_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  if constexpr (pcg::flux1_shared(sizeof(R))) {
+    __shared__ R kcarry[2 * ncorr1<NS>() * 128];
+    int64_t t;
+    const pcg::Seg& sg = seg_of(a, t);
+    switch (sg.variant) {
+      case 0: flux1_x<NS, MIX, EXACT, R>(a, sg, t, kcarry); break;
+      case 1: flux1_march<NS, MIX, EXACT, 1, R>(a, sg, t, kcarry); break;
+      default: flux1_march<NS, MIX, EXACT, 2, R>(a, sg, t, kcarry); break;
+    }
+  } else {
+    Item it;
+    if (!item_of(a, it)) return;
+    switch (it.variant) {
+      case 0: flux1_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+      case 1: flux1_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+      default: flux1_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+    }
   }
 }
 
@@ -851,13 +1047,13 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
 }
 
 // One launch covers the final fluxes of all three directions. The two D-faces of a cell
-// share its transverse correction, so each thread computes one correction per face:
-//  * x-faces: a warp covers 32 consecutive cells of one (j, k) row and solves the 31
-//    faces between them; each lane takes its right neighbour's correction by shuffle;
-//  * y- and z-faces: a warp covers 32 consecutive i of one row and each thread marches
-//    pcg::F2_MARCH faces along D, carrying the correction of the cell behind the face.
-// A block is four such warps (four rows). The per-segment tile counts are computed by
-// flux2_tiles on the host.
+// share its transverse correction, so each thread forms about one correction per face:
+//  * x-faces, one per thread in linear order: the correction right of a face comes from
+//    the next lane's shared-memory slot (the last lane of a warp and the last face of a
+//    row form it themselves);
+//  * y- and z-faces: each thread marches pcg::FACE_MARCH faces along D, carrying the
+//    correction of the cell behind the face.
+// Block counts per segment are pcg::face_tiles on the host.
 template <int NS, bool MIX, bool EXACT, class R>
 __device__ __forceinline__ void flux2_consts(const pcg::StageArgs& a, const pcg::Region& rg, int D, R& cdtdx0,
                                              R& cdtdx1, R& hdt, double& p0d) {
@@ -871,50 +1067,44 @@ __device__ __forceinline__ void flux2_consts(const pcg::StageArgs& a, const pcg:
 }
 
 template <int NS, bool MIX, bool EXACT, class R>
-__device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t) {
+__device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kx) {
   const pcg::Region& rg = a.regions[sg.region];
-  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
-  const int64_t nti = (sg.n[0] + 30) / 31, nr = (sg.n[1] + 3) / 4;
-  const int ti = (int)(t % nti);
-  const int64_t rest = t / nti;
-  const int j = sg.lo[1] + (int)(rest % nr) * 4 + row;
-  const int k = sg.lo[2] + (int)(rest / nr);
-  if (j >= sg.lo[1] + sg.n[1]) return;  // whole warp
-  const int ic = sg.lo[0] - 1 + ti * 31 + lane;  // this lane's cell; faces ic + 1 ...
-  const int ilast = sg.lo[0] + sg.n[0] - 1;      // last face (= last cell needed)
+  const int64_t local = t * blockDim.x + threadIdx.x;
+  const bool active = local < sg.count;
+  const int64_t q = local / sg.n[0];
+  const int i = sg.lo[0] + (int)(local - q * sg.n[0]);
+  const int j = sg.lo[1] + (int)(q % sg.n[1]);
+  const int k = sg.lo[2] + (int)(q / sg.n[1]);
   R cdtdx0, cdtdx1, hdt;
   double p0d;
   flux2_consts<NS, MIX, EXACT, R>(a, rg, 0, cdtdx0, cdtdx1, hdt, p0d);
-  R K[ncorr<NS>()], Kr[ncorr<NS>()];
-  if (ic <= ilast) {
-    flux2_corr<NS, 0, R>(rg, ic, j, k, cdtdx0, cdtdx1, R(p0d), K);
+  const R p0 = R(p0d);
+  R* mine = kx + threadIdx.x;
+  R K[ncorr<NS>()];
+  if (active) {
+    flux2_corr<NS, 0, R>(rg, i - 1, j, k, cdtdx0, cdtdx1, p0, K);
+#pragma unroll
+    for (int n = 0; n < ncorr<NS>(); ++n) mine[n * 128] = K[n];
+  }
+  __syncwarp();
+  if (!active) return;
+  R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+  flux2_state<NS, EXACT, 0, 0, R>(rg, i, j, k, K, hdt, p0, ql);
+  if ((threadIdx.x & 31) == 31 || i == sg.lo[0] + sg.n[0] - 1) {
+    flux2_corr<NS, 0, R>(rg, i, j, k, cdtdx0, cdtdx1, p0, K);
   } else {
 #pragma unroll
-    for (int n = 0; n < ncorr<NS>(); ++n) K[n] = R(0);
+    for (int n = 0; n < ncorr<NS>(); ++n) K[n] = mine[n * 128 + 1];
   }
-#pragma unroll
-  for (int n = 0; n < ncorr<NS>(); ++n) Kr[n] = __shfl_down_sync(0xffffffffu, K[n], 1);
-  const int i = ic + 1;  // face between this lane's cell and the next lane's
-  if (lane == 31 || i > ilast) return;
-  R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
-  flux2_state<NS, EXACT, 0, 0, R>(rg, i, j, k, K, hdt, R(p0d), ql);
-  flux2_state<NS, EXACT, 0, 1, R>(rg, i, j, k, Kr, hdt, R(p0d), qr);
+  flux2_state<NS, EXACT, 0, 1, R>(rg, i, j, k, K, hdt, p0, qr);
   flux2_face<NS, MIX, EXACT, 0, R>(a, rg, i, j, k, ql, qr, p0d);
 }
 
 template <int NS, bool MIX, bool EXACT, int D, class R>
 __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kcarry) {
   const pcg::Region& rg = a.regions[sg.region];
-  constexpr int RA = (D == 1) ? 2 : 1;  // row axis; lanes run along i, the march along D
-  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
-  const int64_t nti = (sg.n[0] + 31) / 32, nr = (sg.n[RA] + 3) / 4;
-  const int ti = (int)(t % nti);
-  const int64_t rest = t / nti;
-  const int r = sg.lo[RA] + (int)(rest % nr) * 4 + row;
-  const int m0 = sg.lo[D] + (int)(rest / nr) * pcg::F2_MARCH;
-  const int i = sg.lo[0] + ti * 32 + lane;
-  if (i >= sg.lo[0] + sg.n[0] || r >= sg.lo[RA] + sg.n[RA]) return;
-  const int m1 = min(m0 + pcg::F2_MARCH, sg.lo[D] + sg.n[D]);
+  int i, r, m0, m1;
+  if (!march_of<D>(sg, t, i, r, m0, m1)) return;
   R cdtdx0, cdtdx1, hdt;
   double p0d;
   flux2_consts<NS, MIX, EXACT, R>(a, rg, D, cdtdx0, cdtdx1, hdt, p0d);
@@ -954,7 +1144,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
   int64_t t;
   const pcg::Seg& sg = seg_of(a, t);
   switch (sg.variant) {
-    case 0: flux2_x<NS, MIX, EXACT, R>(a, sg, t); break;
+    case 0: flux2_x<NS, MIX, EXACT, R>(a, sg, t, kcarry); break;
     case 1: flux2_march<NS, MIX, EXACT, 1, R>(a, sg, t, kcarry); break;
     default: flux2_march<NS, MIX, EXACT, 2, R>(a, sg, t, kcarry); break;
   }

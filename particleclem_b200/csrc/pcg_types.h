@@ -1,6 +1,7 @@
 // pcg_types.h -- layouts shared by the host runtime and the device kernels.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 #if defined(__CUDACC__)
@@ -101,14 +102,18 @@ struct Region {
 // A run of thread blocks of one stage working on one region (and one variant, e.g.
 // a direction or a (direction, other direction) pair) over the index box
 // [lo, lo + n).
-// Final-flux stage tiling (k_flux2): x-faces take 31 faces per 32-lane warp, y- and
-// z-faces march F2_MARCH faces per thread along their direction; four rows per block.
-constexpr int F2_MARCH = 4;
-PCG_HD constexpr int64_t flux2_tiles(int d, const int32_t n[3]) {
-  return d == 0 ? int64_t((n[0] + 30) / 31) * ((n[1] + 3) / 4) * n[2]
-       : d == 1 ? int64_t((n[0] + 31) / 32) * ((n[2] + 3) / 4) * ((n[1] + F2_MARCH - 1) / F2_MARCH)
-                : int64_t((n[0] + 31) / 32) * ((n[1] + 3) / 4) * ((n[2] + F2_MARCH - 1) / F2_MARCH);
+// Blocks (of 128 threads) of the stages that share a cell's transverse correction
+// between its two faces (k_flux1, k_flux2): x-faces one face per thread; y- and
+// z-faces one thread per FACE_MARCH consecutive faces along their direction.
+constexpr int FACE_MARCH = 4;
+PCG_HD constexpr int64_t face_threads(int d, const int32_t n[3]) {
+  return d == 0 ? int64_t(n[0]) * n[1] * n[2]
+                : int64_t(n[0]) * n[d == 1 ? 2 : 1] * ((n[d] + FACE_MARCH - 1) / FACE_MARCH);
 }
+PCG_HD constexpr int64_t face_tiles(int d, const int32_t n[3]) { return (face_threads(d, n) + 127) / 128; }
+// k_flux1 shares corrections in the FP32 form only (element size of the compute type);
+// the FP64 forms run one face per thread.
+PCG_HD constexpr bool flux1_shared(size_t esz) { return esz == 4; }
 
 struct Seg {
   int32_t region;

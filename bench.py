@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--box", type=int, default=32, help="box edge")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline work budget")
+    ap.add_argument("--serve-per-run", type=int, default=4, help="requests per ensemble run in the serving check")
     return ap.parse_args()
 
 
@@ -323,6 +324,19 @@ def run_ours(args):
     e2e_value = world * ncell * kp / (mse / 1e3)
     pipe.close()
 
+    # ---- serving: patch-advance latency under Poisson arrivals with continuous batching
+    # (16 ensemble runs submitting flame boxes of edges 16..64, HBM budget 120 GB)
+    from particleclem_b200.serve import GpuExecutor, Scheduler, serve_sweep
+
+    sp, _ = wl.serving_patches(nruns=16, per_run=args.serve_per_run, seed=5 + rank, eos=lev.eos)
+    sx = GpuExecutor(lev.eos, precision=abi.PREC_MIXED)
+    spids = [sx.add_patch(p) for p in sp]
+    sx.start()
+    Scheduler(sx, int(120e9)).run([sx.request(k, p, 0.0) for k, p in enumerate(spids[:4])])
+    sx.synchronize()
+    serving = serve_sweep(sx, spids, int(120e9), loads=(0.5, 0.9))
+    del sx
+
     # ---- roofline: the dominant kernel (one fused region of the whole level) and the step
     from particleclem_b200 import roofline as rl
 
@@ -356,6 +370,10 @@ def run_ours(args):
                             "level.HostPipeline overlaps step k's compute with the copies of k+1 and k-1",
                     "serial": {"value": e2e_serial, "ms_per_step": mse_serial / ke,
                                "path": "same copies and step, one after another"}},
+            "serving": {"workload": f"16 runs x {args.serve_per_run} flame boxes, edges in {{16..64}}, ns9, mixed",
+                        "budget_gb": 120, "saturated_cell_updates_per_s": serving[0]["cell_updates_per_s"],
+                        "loads": [{k: r[k] for k in ("load", "p50_ms", "p99_ms", "cell_updates_per_s", "batches")}
+                                  for r in serving[1:]]},
             "gpu_launches": LevelStepper.launches_per_step * args.steps,
             "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},

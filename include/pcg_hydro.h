@@ -157,6 +157,13 @@ int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t lo[3], cons
 int pcg_hydro_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes,
                     pcg_stream_t stream);
 
+/* Device bytes a pcg_hydro_boxes call over boxes [lo[3b], hi[3b]] (b < nbox) allocates
+ * for its workspace and launch tables (stream-ordered, freed when the call's work
+ * ends): the admission estimate of a serving loop under an HBM budget. Host only.
+ * No counterpart in the reference (its temporaries come from the AMReX arena). */
+int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t* lo, const int32_t* hi,
+                        int64_t* bytes);
+
 /* pc_estdt_hydro over the valid cells of every box (Source/Timestep.H:51-88), the
  * min over boxes, times cfl (Source/PeleC.cpp:930). dt_out is a DEVICE pointer
  * to one double, written asynchronously. Each box's dx is used. */
@@ -204,10 +211,16 @@ int pcg_plan_info(const pcg_plan* plan, int64_t* workspace_bytes, int32_t* nregi
                   int64_t* blocks_per_stage /* [7] */);
 int pcg_plan_destroy(pcg_plan* plan);
 
+/* One-shot calls take their workspace stream-ordered from a memory pool the library
+ * keeps per device without returning freed memory to the driver between calls. This
+ * returns all but keep_bytes of the pool of CUDA device `device` to the driver (after
+ * the work that used it completes). No counterpart in the reference. */
+int pcg_trim_workspace(int32_t device, int64_t keep_bytes);
+
 /* ---- launch tuning ------------------------------------------------------------- */
 
 /* Each heavy stage (0 ctoprim, 2 trace, 3-5 Riemann stages) exists in three register
- * budgets (variants 0-2: no cap, moderate, tight); the library keeps the variant used
+ * budgets (variants 0-2, increasingly tight); the library keeps the variant used
  * per (precision_mode, nspec, stage). particleclem_b200/autotune.py times them and
  * sets the fastest. No counterpart in the reference (AMReX chooses launch shapes). */
 int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage, int32_t variant);

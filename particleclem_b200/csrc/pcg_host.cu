@@ -3,10 +3,11 @@
 //
 // A launch plan lays out, for every box (region) of a call, the intermediate arrays
 // of the advance in one device workspace and builds per-stage segment tables (see
-// pcg_types.h). One-shot calls allocate the workspace stream-ordered
-// (cudaMallocAsync / cudaFreeAsync on the caller's stream, the role
-// amrex::The_Async_Arena plays in the reference); pcg_plan objects keep it for
-// repeated steps so that a step can be captured in a CUDA graph.
+// pcg_types.h). One-shot calls allocate the workspace stream-ordered on the caller's
+// stream from a memory pool the library owns per device, which keeps its memory
+// between calls (the role amrex::The_Async_Arena plays in the reference);
+// pcg_plan objects keep theirs for repeated steps so that a step can be captured in a
+// CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,6 +56,45 @@ int g_variant[3][2][7] = {
 int variant_of(int prec, int ns, int stage) {
   std::lock_guard<std::mutex> lk(g_var_mu);
   return g_variant[prec][ns == 1 ? 0 : 1][stage];
+}
+
+// Stream-ordered workspace pool per device. Its release threshold is unbounded, so
+// memory freed by one call is reused by the next without returning to the driver (the
+// default pool would trim it at every synchronisation); pcg_trim_workspace hands it back.
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+cudaError_t workspace_pool(cudaMemPool_t* pool) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
+    uint64_t thr = UINT64_MAX;
+    if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr)) != cudaSuccess) {
+      cudaMemPoolDestroy(p);
+      return e;
+    }
+    g_pool[dev] = p;
+  }
+  *pool = g_pool[dev];
+  return cudaSuccess;
+}
+
+cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = workspace_pool(&pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 
 int fail(int code, const char* fmt, ...) {
@@ -404,11 +444,11 @@ int run_once(const pcg_hydro_params* p, std::vector<BoxIn>& boxes, int first, in
   Layout L;
   build_layout(L, boxes, p->nspec, p->precision_mode == PCG_PREC_MIXED);
   void* ws = nullptr;
-  if (L.ws_bytes) CUDA_TRY(cudaMallocAsync(&ws, L.ws_bytes, s));
+  if (L.ws_bytes) CUDA_TRY(ws_alloc(&ws, L.ws_bytes, s));
   rebase_workspace(L, boxes, static_cast<char*>(ws));
   Tables T;
   pack_tables(L, T);
-  cudaError_t e = cudaMallocAsync(&T.dev, T.bytes, s);
+  cudaError_t e = ws_alloc(&T.dev, T.bytes, s);
   if (e != cudaSuccess) {
     if (ws) cudaFreeAsync(ws, s);
     cudaGetLastError();
@@ -648,7 +688,7 @@ int pcg_ctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t 
   Tables T;
   pack_tables(L, T);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  CUDA_TRY(cudaMallocAsync(&T.dev, T.bytes, s));
+  CUDA_TRY(ws_alloc(&T.dev, T.bytes, s));
   cudaError_t e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     bind_tables(T);
@@ -734,6 +774,26 @@ int pcg_hydro_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* bo
   return run_once(prm, bs, K_CTOPRIM, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
 }
 
+int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t* lo, const int32_t* hi,
+                        int64_t* bytes) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  if (nbox < 0 || (nbox > 0 && (!lo || !hi)) || !bytes) return fail(PCG_EINVAL, "bad arguments");
+  std::vector<BoxIn> bs(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    bs[b] = BoxIn{};
+    bs[b].bx = mkbox(lo + 3 * b, hi + 3 * b);
+    if (bs[b].bx.cells() <= 0) return fail(PCG_EINVAL, "empty box %d", b);
+    bs[b].internal_q = true;
+  }
+  Layout L;
+  build_layout(L, bs, prm->nspec, prm->precision_mode == PCG_PREC_MIXED);
+  Tables T;
+  pack_tables(L, T);
+  *bytes = int64_t((L.ws_bytes + kAlign - 1) / kAlign * kAlign + T.bytes);
+  return PCG_OK;
+}
+
 int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl, double* dt_out, pcg_stream_t stream) {
   if (nspec != 1 && nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d", nspec);
   if (nbox <= 0 || !boxes || !dt_out) return fail(PCG_EINVAL, "bad arguments");
@@ -757,7 +817,7 @@ int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl, dou
   std::memcpy(host.data(), ab.data(), b1);
   std::memcpy(host.data() + b1, segs.data(), b2);
   char* dev = nullptr;
-  CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&dev), b1 + b2 + b3, s));
+  CUDA_TRY(ws_alloc(reinterpret_cast<void**>(&dev), b1 + b2 + b3, s));
   cudaError_t e = cudaMemcpyAsync(dev, host.data(), b1 + b2, cudaMemcpyHostToDevice, s);
   rc = PCG_OK;
   if (e == cudaSuccess) {
@@ -807,7 +867,7 @@ int pcg_update_state(int32_t nspec, int32_t nbox, const pcg_box* boxes, const pc
   std::memcpy(host.data(), ab.data(), b1);
   std::memcpy(host.data() + b1, segs.data(), b2);
   char* dev = nullptr;
-  CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&dev), b1 + b2, s));
+  CUDA_TRY(ws_alloc(reinterpret_cast<void**>(&dev), b1 + b2, s));
   cudaError_t e = cudaMemcpyAsync(dev, host.data(), b1 + b2, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     pcg::AuxArgs a{};
@@ -971,6 +1031,15 @@ int pcg_plan_info(const pcg_plan* P, int64_t* workspace_bytes, int32_t* nregions
   if (nregions) *nregions = (int32_t)P->L.regions.size();
   if (blocks_per_stage)
     for (int s = 0; s < K_NSTAGE; ++s) blocks_per_stage[s] = P->L.nblocks[s];
+  return PCG_OK;
+}
+
+int pcg_trim_workspace(int32_t device, int64_t keep_bytes) {
+  if (device < 0 || device >= kMaxDevices || keep_bytes < 0) return fail(PCG_EINVAL, "bad arguments");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[device]) return PCG_OK;
+  const cudaError_t e = cudaMemPoolTrimTo(g_pool[device], size_t(keep_bytes));
+  if (e != cudaSuccess) return fail(PCG_ECUDA, "pool trim: %s", cudaGetErrorString(e));
   return PCG_OK;
 }
 

@@ -100,6 +100,16 @@ def hydro_boxes(prm, boxes, stream=None):
     native.call("pcg_hydro_boxes", C.byref(prm), len(boxes), arr, _stream_ptr(stream))
 
 
+def workspace_bytes(prm, extents):
+    """Device bytes hydro_boxes allocates for boxes given as (lo, hi) pairs (host only)."""
+    n = len(extents)
+    lo = (C.c_int32 * (3 * n))(*[int(v) for l, _ in extents for v in l])
+    hi = (C.c_int32 * (3 * n))(*[int(v) for _, h in extents for v in h])
+    out = C.c_int64()
+    native.call("pcg_hydro_workspace", C.byref(prm), n, lo, hi, C.byref(out))
+    return out.value
+
+
 def estdt(nspec, boxes, cfl, dt_out, stream=None):
     """dt_out: a CUDA float64 tensor of one element."""
     arr = box_array(boxes)

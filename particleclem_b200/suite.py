@@ -1,0 +1,207 @@
+"""Measurement driver for the workloads beside the headline level step.
+
+  python -m particleclem_b200.suite batch   512 independent flame boxes, edges log-uniform
+                                            in [8, 64] per axis (9 species): one batched step
+                                            (13 launches, CUDA graph), mixed and plain FP64,
+                                            per-component error of mixed against FP64
+  python -m particleclem_b200.suite sweep   256^3 periodic turbulence in 64 boxes of 64^3
+                                            (gamma law): PPM and PLM x {FP64, mixed}, error
+                                            growth of mixed against FP64 over the steps
+  python -m particleclem_b200.suite serve   16 ensemble runs submitting flame boxes with
+                                            edges in {16,24,32,48,64}: saturated throughput
+                                            and p50/p99 latency under Poisson arrivals at
+                                            10..100 % of it, HBM admission budget
+
+Each prints one JSON line per result. All inputs are synthetic (seeded generators of
+particleclem_b200.workloads). The plain FP64 form is bit-identical to the CPU
+restatement of the reference (the GPU parity tests), so errors against it are errors
+against the reference arithmetic.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+from . import abi, roofline as rl, workloads as wl
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _timed(torch, fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _rel(torch, a, b):
+    """Per-component relative L1 and Linf of b against a (component-major tensors)."""
+    d = (a - b).abs().reshape(a.shape[0], -1)
+    r = a.abs().reshape(a.shape[0], -1)
+    l1 = (d.sum(1) / r.sum(1).clamp_min(1e-300)).cpu().numpy()
+    li = (d.max(1).values / r.max(1).values.clamp_min(1e-300)).cpu().numpy()
+    return l1, li
+
+
+def run_batch(args):
+    import torch
+
+    from .batch import BoxBatch
+
+    eos = wl.load_nasa7()
+    patches = wl.flame_boxes(args.nbox, seed=3, eos=eos, lo=8, hi=64)
+    ncell = sum(p.ncells for p in patches)
+    pk = rl.peaks(ROOT)
+    edges = [[p.hi[d] - p.lo[d] + 1 for d in range(3)] for p in patches]
+    balg = sum(rl.b_alg_box(e, 9) for e in edges)
+    res = {}
+    states = {}
+    for name, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+        bb = BoxBatch(patches, eos, precision=prec)
+        bb.step()  # one step from the initial state, kept for the error
+        torch.cuda.synchronize()
+        states[name] = [s.data.clone() for s in bb.states]
+        bb.capture()
+        ms = _timed(torch, bb.replay, args.steps, args.warmup)
+        res[name] = {"ms_per_step": ms, "cell_updates_per_s": ncell / (ms / 1e3),
+                     "path_hbm_frac": balg / (ms / 1e3) / 1e9 / pk["hbm_gbs"]}
+        bb.close()
+        del bb
+        torch.cuda.empty_cache()
+    g = abi.NGROW
+    num = torch.zeros(abi.nvar(9), dtype=torch.float64, device="cuda")
+    den = torch.zeros_like(num)
+    mx_d = torch.zeros_like(num)
+    mx_r = torch.zeros_like(num)
+    for a, b in zip(states["fp64"], states["mixed"]):
+        a = a[:, g:-g, g:-g, g:-g].reshape(a.shape[0], -1)
+        b = b[:, g:-g, g:-g, g:-g].reshape(b.shape[0], -1)
+        num += (a - b).abs().sum(1)
+        den += a.abs().sum(1)
+        mx_d = torch.maximum(mx_d, (a - b).abs().max(1).values)
+        mx_r = torch.maximum(mx_r, a.abs().max(1).values)
+    l1 = (num / den.clamp_min(1e-300)).cpu().numpy()
+    li = (mx_d / mx_r.clamp_min(1e-300)).cpu().numpy()
+    out = {"workload": f"flame_boxes_{args.nbox}_loguniform_8_64_ns9", "boxes": args.nbox, "cells": ncell,
+           "mixed": res["mixed"], "fp64": res["fp64"], "speedup_mixed_over_fp64": res["fp64"]["ms_per_step"] /
+           res["mixed"]["ms_per_step"], "error_mixed_vs_fp64_one_step": {"max_rel_l1": float(l1.max()),
+                                                                        "max_rel_linf": float(li.max())},
+           "launches_per_step": 10, "b_alg_bytes_per_step": balg, "peak_source": pk["source"]}
+    print(json.dumps(out), flush=True)
+
+
+def run_sweep(args):
+    import torch
+
+    from .level import LevelStepper
+
+    lev0 = wl.turbulence(n=args.n, box=args.box, seed=4)
+    for ppm in (1, 0):
+        a = LevelStepper(lev0, precision=abi.PREC_FP64, fuse=False, ppm_type=ppm)
+        b = LevelStepper(lev0, precision=abi.PREC_MIXED, fuse=True, ppm_type=ppm)
+        ms_a = _timed(torch, a.step, 3, 1)
+        ms_b = _timed(torch, b.step, 3, 1)
+        a.state.data.copy_(torch.from_numpy(lev0.state).to(a.dev))
+        b.state.data.copy_(a.state.data)
+        growth = []
+        g = abi.NGROW
+        for s in range(1, args.steps + 1):
+            a.fill()
+            a.plan.estdt(a.cfl, a.dt)
+            a.plan.hydro(a.dt)
+            a.plan.update(a.dt)
+            b.fill()
+            b.dt.copy_(a.dt)  # the same timestep sequence: the difference is precision only
+            b.plan.hydro(b.dt)
+            b.plan.update(b.dt)
+            if s in (1, 2, 5) or s % args.every == 0:
+                l1, li = _rel(torch, a.state.data[:, g:-g, g:-g, g:-g], b.state.data[:, g:-g, g:-g, g:-g])
+                growth.append({"step": s, "max_rel_l1": float(l1[:5].max()), "max_rel_linf": float(li[:5].max())})
+        out = {"workload": f"turbulence_{args.n}^3_as_{args.box}^3_boxes_ns1_mach0.3", "scheme": "PPM" if ppm else "PLM",
+               "fp64_ms_per_step": ms_a, "mixed_ms_per_step": ms_b,
+               "fp64_cell_updates_per_s": lev0.ncells() / (ms_a / 1e3),
+               "mixed_cell_updates_per_s": lev0.ncells() / (ms_b / 1e3),
+               "error_components": "rho, rho u, rho v, rho w, rho E", "growth": growth}
+        print(json.dumps(out), flush=True)
+        a.close()
+        b.close()
+        del a, b
+        torch.cuda.empty_cache()
+
+
+def run_serve(args):
+    import torch
+
+    from .serve import GpuExecutor, Scheduler, serve_sweep
+
+    eos = wl.load_nasa7()
+    patches, runs = wl.serving_patches(nruns=args.runs, per_run=args.per_run, seed=5, eos=eos)
+    budget = int(args.budget_gb * 1e9)
+    ex = GpuExecutor(eos, precision=abi.PREC_MIXED)
+    pids = [ex.add_patch(p) for p in patches]
+    # warm the library and the stream-ordered memory pool
+    ex.start()
+    Scheduler(ex, budget).run([ex.request(k, p, 0.0) for k, p in enumerate(pids[:8])])
+    ex.synchronize()
+    res = serve_sweep(ex, pids, budget, loads=tuple(args.loads))
+    # mixed-precision error of the served hydro sources against the plain FP64 form
+    ex64 = GpuExecutor(eos, precision=abi.PREC_FP64)
+    sample = pids[: args.error_sample]
+    for k in sample:
+        ex64.add_patch(patches[k])
+    ex64.start()
+    Scheduler(ex64, budget).run([ex64.request(i, i, 0.0) for i in range(len(sample))])
+    ex64.synchronize()
+    worst_src, worst_state = 0.0, 0.0
+    g = abi.NGROW
+    for i, k in enumerate(sample):
+        # same dt for both forms (each patch's estTimeStep is FP64 in both)
+        l1, _ = _rel(torch, ex64.outs[i].data, ex.outs[k].data)
+        worst_src = max(worst_src, float(l1.max()))
+        dt = ex64.boxes[i].dt
+        s_old = ex64.states[i].data[:, g:-g, g:-g, g:-g]
+        l1s, _ = _rel(torch, s_old + dt * ex64.outs[i].data, s_old + dt * ex.outs[k].data)
+        worst_state = max(worst_state, float(l1s.max()))
+    for r in res:
+        r.update({"workload": f"serving_{args.runs}runs_x{args.per_run}_flame_boxes_16-64_ns9",
+                  "budget_gb": args.budget_gb, "precision": "mixed"})
+        print(json.dumps(r), flush=True)
+    print(json.dumps({"serving_error_mixed_vs_fp64": {"sample": len(sample), "s_new_max_rel_l1": worst_state,
+                                                      "hydro_source_max_rel_l1": worst_src}}), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    b = sub.add_parser("batch")
+    b.add_argument("--nbox", type=int, default=512)
+    b.add_argument("--steps", type=int, default=10)
+    b.add_argument("--warmup", type=int, default=3)
+    s = sub.add_parser("sweep")
+    s.add_argument("--n", type=int, default=256)
+    s.add_argument("--box", type=int, default=64)
+    s.add_argument("--steps", type=int, default=100)
+    s.add_argument("--every", type=int, default=10)
+    v = sub.add_parser("serve")
+    v.add_argument("--runs", type=int, default=16)
+    v.add_argument("--per-run", type=int, default=32)
+    v.add_argument("--budget-gb", type=float, default=120.0)
+    v.add_argument("--loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.9, 1.0])
+    v.add_argument("--error-sample", type=int, default=32)
+    args = ap.parse_args(argv)
+    {"batch": run_batch, "sweep": run_sweep, "serve": run_serve}[args.cmd](args)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

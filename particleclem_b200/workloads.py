@@ -258,6 +258,22 @@ def flame_boxes(nbox=512, seed=3, eos=None, lo=8, hi=64):
     return [flame_patch(e, seed * 100003 + b, eos) for b, e in enumerate(edges)]
 
 
+def serving_patches(nruns=16, per_run=32, seed=5, eos=None, edges=(16, 24, 32, 48, 64)):
+    """Requests of an ensemble of ``nruns`` runs: each run submits ``per_run`` flame
+    boxes whose edges are drawn uniformly from ``edges`` per axis (run-seeded), each
+    with its own front offset. Returned in submission order (runs interleaved) with
+    the run of each."""
+    eos = eos or load_nasa7()
+    rngs = [np.random.default_rng(seed * 1000 + r) for r in range(nruns)]
+    patches, runs = [], []
+    for k in range(per_run):
+        for r in range(nruns):
+            e = rngs[r].choice(np.asarray(edges), size=3)
+            patches.append(flame_patch(e, seed * 100003 + r * 1009 + k, eos))
+            runs.append(r)
+    return patches, runs
+
+
 # ------------------------------------------------------------------ turbulence (config 4)
 def turbulence(n=256, box=64, seed=4, kmax=32, mach=0.3, gamma=1.4) -> Level:
     eos = GammaLaw(gamma=gamma)

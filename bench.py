@@ -197,28 +197,69 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # each rank advances its own level (independent ensemble member, seed per rank)
-    lev = wl.flame(n=args.n, box=args.box, seed=2 + rank)
-    ncell = lev.ncells()
+    # ---- headline: batched mixed form, fused plan, CUDA graphs. One GPU: the 128^3 level.
+    # N GPUs: one level of n x n x (n*N) cut into z-slabs of n^3, one per rank, with the
+    # 4-cell halo exchange (NCCL send/recv) and the dt all-reduce-min every step.
+    if world == 1:
+        lev = wl.flame(n=args.n, box=args.box, seed=2)
+        st = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
+        st.step()  # valid dt and intermediates for the launch-shape autotuner
+        tuned = {"mixed": autotune.tune(st.plan, st.dt, reps=3)}
+        st.capture()
+        step_fn = st.replay
+        parallelism = "single GPU"
+    else:
+        from particleclem_b200.slab import DistComm, SlabStepper, step as slab_step
 
-    # ---- headline: batched mixed form, fused plan, one CUDA graph per step
-    st = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
-    st.step()  # valid dt and intermediates for the launch-shape autotuner
-    tuned = {"mixed": autotune.tune(st.plan, st.dt, reps=3)}
-    st.capture()
+        slab = wl.flame_slab(n=args.n, nz=args.n * world, nranks=world, rank=rank, box=args.box, seed=2)
+        st = SlabStepper(slab, world, rank, precision=abi.PREC_MIXED, fuse=True)
+        st.fill()
+        st.plan.estdt(st.cfl, st.dt)  # a local dt for the launch-shape autotuner
+        tuned = {"mixed": autotune.tune(st.plan, st.dt, reps=3)}
+        st.capture()  # leaves the slab's state as generated
+        comm = DistComm()
+
+        def step_fn():
+            slab_step([st], comm)
+
+        parallelism = (f"z-slabs x{world}: one {args.n}x{args.n}x{args.n * world} level, {args.n}^3 per GPU, "
+                       "4-cell halo exchange (NCCL send/recv) + dt all-reduce-min every step")
+    ncell = st.ncells
     for _ in range(args.warmup):
-        st.replay()
+        step_fn()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     with ClockSampler(local) as clk:
         e0.record()
         for _ in range(args.steps):
-            st.replay()
+            step_fn()
         e1.record()
         barrier()
     ms = max_over_ranks(e0.elapsed_time(e1))
     clocks = clk.summary()
     value = world * ncell * args.steps / (ms / 1e3)
+    if world > 1:
+        # end to end for the decomposed level: every step uploads each slab's state from
+        # pinned host memory, steps (with the exchange) and downloads it
+        host_in = torch.from_numpy(slab.state).pin_memory()
+        host_out1 = torch.empty_like(host_in).pin_memory()
+        h2d = d2h = host_in.numel() * 8
+        for _ in range(2):
+            st.state.data.copy_(host_in, non_blocking=True)
+            step_fn()
+            host_out1.copy_(st.state.data, non_blocking=True)
+        barrier()
+        kp = ke = max(2, min(args.steps, 5))
+        e0.record()
+        for _ in range(kp):
+            st.state.data.copy_(host_in, non_blocking=True)
+            step_fn()
+            host_out1.copy_(st.state.data, non_blocking=True)
+        e1.record()
+        barrier()
+        mse = mse_serial = max_over_ranks(e0.elapsed_time(e1))
+        e2e_value = e2e_serial = world * ncell * kp / (mse / 1e3)
+        lev = wl.flame(n=args.n, box=args.box, seed=2 + rank)  # per-GPU level for the side measurements
 
     # ---- per-stage CUDA-event timings of the same step (not graph-captured)
     names = ["fill", "estdt"] + ["hydro." + s for s in hydro.Plan.STAGES] + ["update"]
@@ -285,44 +326,45 @@ def run_ours(args):
     # upload of step k+1 and the download of step k-1 overlap the step k).
     from particleclem_b200.level import HostPipeline
 
-    lev_e = wl.flame(n=args.n, box=args.box, seed=2 + rank)
-    host_in = torch.from_numpy(lev_e.state).pin_memory()
-    host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
-    h2d = host_in.numel() * 8
-    d2h = host_out[0].numel() * 8
-    se = LevelStepper(lev_e, precision=abi.PREC_MIXED, fuse=True)
-    for _ in range(2):
-        se.state.data.copy_(host_in, non_blocking=True)
-        se.step()
-        host_out[0].copy_(se.state.data, non_blocking=True)
-    barrier()
-    ke = max(1, min(args.steps, 5))
-    e0.record()
-    for _ in range(ke):
-        se.state.data.copy_(host_in, non_blocking=True)
-        se.step()
-        host_out[0].copy_(se.state.data, non_blocking=True)
-    e1.record()
-    barrier()
-    mse_serial = max_over_ranks(e0.elapsed_time(e1))
-    e2e_serial = world * ncell * ke / (mse_serial / 1e3)
-    se.close()
+    lev_e = wl.flame(n=args.n, box=args.box, seed=2 + rank) if world == 1 else None
+    if world == 1:
+        host_in = torch.from_numpy(lev_e.state).pin_memory()
+        host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
+        h2d = host_in.numel() * 8
+        d2h = host_out[0].numel() * 8
+        se = LevelStepper(lev_e, precision=abi.PREC_MIXED, fuse=True)
+        for _ in range(2):
+            se.state.data.copy_(host_in, non_blocking=True)
+            se.step()
+            host_out[0].copy_(se.state.data, non_blocking=True)
+        barrier()
+        ke = max(1, min(args.steps, 5))
+        e0.record()
+        for _ in range(ke):
+            se.state.data.copy_(host_in, non_blocking=True)
+            se.step()
+            host_out[0].copy_(se.state.data, non_blocking=True)
+        e1.record()
+        barrier()
+        mse_serial = max_over_ranks(e0.elapsed_time(e1))
+        e2e_serial = world * ncell * ke / (mse_serial / 1e3)
+        se.close()
 
-    pipe = HostPipeline(lev_e, depth=2, precision=abi.PREC_MIXED, fuse=True)
-    for i in range(3):
-        pipe.submit(host_in, host_out[i % 2])
-    pipe.synchronize()
-    barrier()
-    kp = max(2, args.steps)
-    e0.record(pipe.up)
-    for i in range(kp):
-        pipe.submit(host_in, host_out[i % 2])
-    e1.record(pipe.down)
-    pipe.synchronize()
-    barrier()
-    mse = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * ncell * kp / (mse / 1e3)
-    pipe.close()
+        pipe = HostPipeline(lev_e, depth=2, precision=abi.PREC_MIXED, fuse=True)
+        for i in range(3):
+            pipe.submit(host_in, host_out[i % 2])
+        pipe.synchronize()
+        barrier()
+        kp = max(2, args.steps)
+        e0.record(pipe.up)
+        for i in range(kp):
+            pipe.submit(host_in, host_out[i % 2])
+        e1.record(pipe.down)
+        pipe.synchronize()
+        barrier()
+        mse = max_over_ranks(e0.elapsed_time(e1))
+        e2e_value = world * ncell * kp / (mse / 1e3)
+        pipe.close()
 
     # ---- serving: patch-advance latency under Poisson arrivals with continuous batching
     # (16 ensemble runs submitting flame boxes of edges 16..64, HBM budget 120 GB)
@@ -358,23 +400,27 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "cells_per_gpu": ncell, "boxes_per_gpu": len(lev.boxes),
                        "form": "batched mixed precision, boxes fused into one region, CUDA graph per step",
-                       "parallelism": f"replicas x{world} (independent level per GPU)" if world > 1 else "single GPU",
+                       "parallelism": parallelism,
                        "l2": "inputs larger than L2 (state 0.34 GB, intermediates 3.4 GB per step)"},
             "fp64_dropin": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms64 / k64,
-                            "form": "plain FP64, reference operation order, per-box (64 boxes), CUDA graph",
+                            "form": "plain FP64, reference operation order, per-box (64 boxes), CUDA graph"
+                                    + (", one level per GPU" if world > 1 else ""),
                             "speedup_of_mixed": value / fp64_value},
             "error_vs_fp64": err,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": mse / kp, "steps": kp,
-                    "path": "pinned host state -> H2D -> fill/estdt/hydro/update via C ABI -> D2H, every step; "
-                            "level.HostPipeline overlaps step k's compute with the copies of k+1 and k-1",
+                    "path": ("pinned host state -> H2D -> fill/estdt/hydro/update via C ABI -> D2H, every step; "
+                             "level.HostPipeline overlaps step k's compute with the copies of k+1 and k-1")
+                            if world == 1 else
+                            "per rank: pinned host slab -> H2D -> slab step with halo exchange and dt all-reduce "
+                            "-> D2H, every step",
                     "serial": {"value": e2e_serial, "ms_per_step": mse_serial / ke,
                                "path": "same copies and step, one after another"}},
             "serving": {"workload": f"16 runs x {args.serve_per_run} flame boxes, edges in {{16..64}}, ns9, mixed",
                         "budget_gb": 120, "saturated_cell_updates_per_s": serving[0]["cell_updates_per_s"],
                         "loads": [{k: r[k] for k in ("load", "p50_ms", "p99_ms", "cell_updates_per_s", "batches")}
                                   for r in serving[1:]]},
-            "gpu_launches": LevelStepper.launches_per_step * args.steps,
+            "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 3, estdt 2, hydro 7, update 1
             "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},
             "roofline": roof,

@@ -212,6 +212,77 @@ def flame(n=128, box=32, seed=2, eos=None) -> Level:
 
 
 @dataclass
+class Slab:
+    """The z-slab [k0, k1] of a level decomposed over ranks: the level's global domain
+    and boundary conditions, the state on grow(slab, NG) and the boxes tiling the slab."""
+
+    eos: object
+    dx: tuple
+    domlo: tuple  # global domain
+    domhi: tuple
+    bclo: tuple
+    bchi: tuple
+    periodic: tuple
+    k0: int
+    k1: int
+    state: np.ndarray  # (NVAR, k1-k0+1+2NG, NY+2NG, NX+2NG)
+    boxes: list = field(default_factory=list)
+
+    @property
+    def nspec(self):
+        return self.eos.nspec
+
+    @property
+    def lo(self):
+        return (self.domlo[0] - NG, self.domlo[1] - NG, self.k0 - NG)
+
+    def ncells(self):
+        return sum(int(np.prod([h - l + 1 for l, h in zip(lo, hi)])) for lo, hi in self.boxes)
+
+
+def slab_range(nz, nranks, rank, box):
+    """k-range of rank's slab: equal slabs, each a whole number of boxes."""
+    if nz % nranks or (nz // nranks) % box:
+        raise ValueError(f"{nz} cells in z do not split into {nranks} slabs of whole {box}-boxes")
+    nzl = nz // nranks
+    return rank * nzl, (rank + 1) * nzl - 1
+
+
+def split_level(lev: Level, nranks, rank, box) -> Slab:
+    """Rank's slab of an existing level (ghost cells included, as the level holds them)."""
+    nz = lev.domhi[2] - lev.domlo[2] + 1
+    k0, k1 = slab_range(nz, nranks, rank, box)
+    k0 += lev.domlo[2]
+    k1 += lev.domlo[2]
+    st = lev.state[:, k0 - lev.domlo[2]:k1 - lev.domlo[2] + 1 + 2 * NG]
+    boxes = [b for b in lev.boxes if b[0][2] >= k0 and b[1][2] <= k1]
+    return Slab(lev.eos, lev.dx, lev.domlo, lev.domhi, lev.bclo, lev.bchi, lev.periodic, k0, k1,
+                np.ascontiguousarray(st), boxes)
+
+
+def flame_slab(n=128, nz=256, nranks=2, rank=0, box=32, seed=2, eos=None) -> Slab:
+    """Rank's slab of the flame level of edges (n, n, nz): periodic x/y, outflow z, the
+    front wrinkled around z = nz*dx/2; the velocity noise is drawn per rank."""
+    eos = eos or load_nasa7()
+    k0, k1 = slab_range(nz, nranks, rank, box)
+    L = n * FLAME_DX
+    Lz = nz * FLAME_DX
+    phx, phy = np.random.default_rng(seed).uniform(0, 2 * np.pi, size=2)
+    rng = np.random.default_rng(seed * 7919 + rank)
+    c = (np.arange(n + 2 * NG) - NG + 0.5) * FLAME_DX
+    cz = (np.arange(k0 - NG, k1 + NG + 1) + 0.5) * FLAME_DX
+    Zc, Yc, Xc = np.meshgrid(cz, c, c, indexing="ij")
+    zf = 0.5 * Lz + 0.02 * L * np.sin(2 * np.pi * Xc / L + phx) * np.cos(2 * np.pi * Yc / L + phy)
+    rho, u, v, w, p, Y = _flame_prims(eos, Xc, Yc, Zc, zf, rng, L)
+    U = conserved_from_prim(eos, rho, u, v, w, p, Y)
+    boxes = [((b[0][0], b[0][1], b[0][2] + k0), (b[1][0], b[1][1], b[1][2] + k0))
+             for b in tile_boxes((n, n, k1 - k0 + 1), (box, box, box))]
+    return Slab(eos, (FLAME_DX,) * 3, (0, 0, 0), (n - 1, n - 1, nz - 1),
+                (abi.BC_INTERIOR, abi.BC_INTERIOR, abi.BC_OUTFLOW), (abi.BC_INTERIOR, abi.BC_INTERIOR, abi.BC_OUTFLOW),
+                (True, True, False), k0, k1, np.ascontiguousarray(U), boxes)
+
+
+@dataclass
 class Patch:
     """An independent box: its own grown state FAB, no physical boundaries."""
 

@@ -1048,7 +1048,31 @@ static void transdd(int i, int j, int k, int dir, fab_t* qm, fab_t* qp, const fa
 }
 
 /* ---------------------------------------------------------------- umeth */
-/* Source/Godunov.cpp:59-476 (pc_umeth_3D), regular geometry, no inflow/user BC. */
+/* Source/Godunov.cpp:6-55 (pc_low_order_boundary): the idir-fluxes on the face box bfbx
+ * (one plane at a domain boundary) recomputed from PLM states of the two adjacent cells,
+ * without transverse terms (the boundary state is given at time n). */
+static void low_order_boundary(box_t bfbx, int bclo, int bchi, int domlo, int domhi, int plm_iorder,
+                               int use_flattening, int idir, double dx, double dt, const fab_t* q,
+                               const fab_t* qa, fab_t* flx, fab_t* qdir) {
+  box_t bdbx = bfbx;
+  bdbx.hi[idir] -= 1; /* enclosedCells */
+  bdbx = bgrow_dir(bdbx, idir, 1);
+  const box_t bdbx2 = bgrow_hi(bdbx, idir, 1);
+  fab_t qbm = fab_new(bdbx2, QVAR), qbp = fab_new(bdbx, QVAR);
+  double slope[MAXQ];
+  FOR_BOX(bdbx, i, j, k) {
+    double flat = 1.0;
+    if (use_flattening)
+      for (int df = 0; df < 3; df++) flat = dmin(flat, flatten(i, j, k, df, q));
+    for (int n = 0; n < QVAR; ++n) slope[n] = plm_slope(i, j, k, n, idir, q, flat, plm_iorder);
+    pc_plm_d(i, j, k, idir, &qbm, &qbp, slope, q, F(*qa, i, j, k, QC), dx, dt);
+  }
+  FOR_BOX(bfbx, i, j, k) cmpflx(i, j, k, bclo, bchi, domlo, domhi, &qbm, &qbp, flx, qdir, qa, idir);
+  fab_free(&qbm);
+  fab_free(&qbp);
+}
+
+/* Source/Godunov.cpp:59-476 (pc_umeth_3D), regular geometry. */
 static int umeth_3d(box_t bx, const int* bclo, const int* bchi, const int* domlo, const int* domhi,
                     const fab_t* q, const fab_t* qaux, const fab_t* srcQ, fab_t* flx, fab_t* qec,
                     const fab_t* a, fab_t* pdivu, const fab_t* vol, const double* del, double dt,
@@ -1124,6 +1148,23 @@ static int umeth_3d(box_t bx, const int* bclo, const int* bchi, const int* domlo
     const box_t fbx = bnodes(bx, d);
     FOR_BOX(fbx, i, j, k)
       cmpflx(i, j, k, bclo[d], bchi[d], domlo[d], domhi[d], &qmf, &qpf, &flx[d], &qec[d], qaux, d);
+  }
+  /* Source/Godunov.cpp:440-468: faces on inflow / user_bc domain boundaries */
+  for (int d = 0; d < 3; ++d) {
+    if (bclo[d] == BC_INFLOW || bclo[d] == BC_USER) {
+      box_t bfbx = bnodes(bx, d);
+      bfbx.hi[d] = domlo[d];
+      if (bfbx.lo[d] <= bfbx.hi[d])
+        low_order_boundary(bfbx, bclo[d], bchi[d], domlo[d], domhi[d], plm_iorder, use_flattening, d, del[d], dt, q,
+                           qaux, &flx[d], &qec[d]);
+    }
+    if (bchi[d] == BC_INFLOW || bchi[d] == BC_USER) {
+      box_t bfbx = bnodes(bx, d);
+      bfbx.lo[d] = domhi[d] + 1;
+      if (bfbx.lo[d] <= bfbx.hi[d])
+        low_order_boundary(bfbx, bclo[d], bchi[d], domlo[d], domhi[d], plm_iorder, use_flattening, d, del[d], dt, q,
+                           qaux, &flx[d], &qec[d]);
+    }
   }
   /* p div(u), Source/Godunov.H:1033-1060 */
   FOR_BOX(bx, i, j, k) {

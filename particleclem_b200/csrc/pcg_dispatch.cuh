@@ -31,6 +31,9 @@ static cudaError_t launch_v(int stage, const pcg::StageArgs& a, const dim3& grid
     case K_FLUX1: k_flux1<NS, MIX, kExact, R, kMinBlocks[K_FLUX1][V]><<<grid, block, 0, s>>>(a); break;
     case K_FLUX2: k_flux2<NS, MIX, kExact, R, kMinBlocks[K_FLUX2][V]><<<grid, block, 0, s>>>(a); break;
     case K_CONSUP: k_consup<NS, MIX><<<grid, block, 0, s>>>(a); break;
+    case K_LOWBC:
+      if (V == 0) k_lowbc<NS, MIX, kExact, R><<<grid, block, 0, s>>>(a);
+      break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -38,6 +38,9 @@ cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks
 namespace {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
+// launches that are not stages of their own: the low-order inflow/user_bc faces, run as
+// part of stage K_FLUX2 right after it
+enum { K_LOWBC = K_NSTAGE, K_NKIND };
 enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL };
 constexpr int kThreads = 128;
 constexpr size_t kAlign = 256;
@@ -220,8 +223,8 @@ int check_box_common(const IBox& bx, const double* dx, double dt, const int32_t*
   if (!bx.ok()) return fail(PCG_EINVAL, "empty box");
   for (int d = 0; d < 3; ++d) {
     if (!(dx[d] > 0.0) || !std::isfinite(dx[d])) return fail(PCG_EINVAL, "dx[%d] must be positive", d);
-    if (bclo[d] == PCG_BC_INFLOW || bclo[d] == PCG_BC_USER || bchi[d] == PCG_BC_INFLOW || bchi[d] == PCG_BC_USER)
-      return fail(PCG_EUNSUPPORTED, "inflow/user_bc boundaries (pc_low_order_boundary) are not implemented");
+    if (bclo[d] < PCG_BC_INTERIOR || bclo[d] > PCG_BC_USER || bchi[d] < PCG_BC_INTERIOR || bchi[d] > PCG_BC_USER)
+      return fail(PCG_EINVAL, "unknown boundary type in direction %d", d);
   }
   if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(PCG_EINVAL, "dt must be finite and >= 0");
   return PCG_OK;
@@ -243,8 +246,8 @@ struct Layout {
   size_t esz = 8;  // compute-type size of the intermediates
   size_t ws_bytes = 0;
   std::vector<pcg::Region> regions;
-  std::vector<pcg::Seg> segs[K_NSTAGE];
-  int64_t nblocks[K_NSTAGE] = {};
+  std::vector<pcg::Seg> segs[K_NKIND];
+  int64_t nblocks[K_NKIND] = {};
 };
 
 size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v) {
@@ -353,6 +356,22 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool singl
       take(L, fb, 2, fsz, R.qec[d]);
       add_seg(L, K_FLUX2, (int)r, d, fb);
     }
+    // Source/Godunov.cpp:440-468: faces of the box on an inflow or user_bc domain
+    // boundary get their final fluxes again from PLM states without transverse terms
+    for (int d = 0; d < 3; ++d) {
+      const bool lo_bc = (B.bclo[d] == PCG_BC_INFLOW || B.bclo[d] == PCG_BC_USER) && B.bx.lo[d] <= B.domlo[d];
+      const bool hi_bc = (B.bchi[d] == PCG_BC_INFLOW || B.bchi[d] == PCG_BC_USER) && B.bx.hi[d] + 1 >= B.domhi[d] + 1;
+      if (lo_bc) {
+        IBox fb = nodes(B.bx, d);
+        fb.hi[d] = B.domlo[d];
+        if (fb.ok()) add_seg(L, K_LOWBC, (int)r, d, fb);
+      }
+      if (hi_bc) {
+        IBox fb = nodes(B.bx, d);
+        fb.lo[d] = B.domhi[d] + 1;
+        if (fb.ok()) add_seg(L, K_LOWBC, (int)r, d, fb);
+      }
+    }
     add_seg(L, K_CONSUP, (int)r, 0, B.bx);
     L.regions.push_back(R);
   }
@@ -387,14 +406,14 @@ struct Tables {
   void* dev = nullptr;
   size_t bytes = 0;
   const pcg::Region* regions = nullptr;
-  const pcg::Seg* segs[K_NSTAGE] = {};
+  const pcg::Seg* segs[K_NKIND] = {};
   std::vector<char> host;
 };
 
 void pack_tables(const Layout& L, Tables& T) {
   size_t off = L.regions.size() * sizeof(pcg::Region);
-  size_t seg_off[K_NSTAGE];
-  for (int s = 0; s < K_NSTAGE; ++s) {
+  size_t seg_off[K_NKIND];
+  for (int s = 0; s < K_NKIND; ++s) {
     off = (off + 15) / 16 * 16;
     seg_off[s] = off;
     off += L.segs[s].size() * sizeof(pcg::Seg);
@@ -402,37 +421,45 @@ void pack_tables(const Layout& L, Tables& T) {
   T.bytes = std::max<size_t>(off, 16);
   T.host.assign(T.bytes, 0);
   if (!L.regions.empty()) std::memcpy(T.host.data(), L.regions.data(), L.regions.size() * sizeof(pcg::Region));
-  for (int s = 0; s < K_NSTAGE; ++s)
+  for (int s = 0; s < K_NKIND; ++s)
     if (!L.segs[s].empty()) std::memcpy(T.host.data() + seg_off[s], L.segs[s].data(), L.segs[s].size() * sizeof(pcg::Seg));
   // device pointers are filled in by bind_tables once T.dev exists
-  for (int s = 0; s < K_NSTAGE; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(seg_off[s]);
+  for (int s = 0; s < K_NKIND; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(seg_off[s]);
 }
 
 void bind_tables(Tables& T) {
   char* base = static_cast<char*>(T.dev);
   T.regions = reinterpret_cast<const pcg::Region*>(base);
-  for (int s = 0; s < K_NSTAGE; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(base + reinterpret_cast<size_t>(T.segs[s]));
+  for (int s = 0; s < K_NKIND; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(base + reinterpret_cast<size_t>(T.segs[s]));
+}
+
+int launch_kind(const Layout& L, const Tables& T, const pcg_hydro_params* p, int kind, const double* dt_dev,
+                cudaStream_t s) {
+  if (L.nblocks[kind] == 0) return PCG_OK;
+  const bool single = p->precision_mode == PCG_PREC_MIXED;
+  pcg::StageArgs a{};
+  a.regions = T.regions;
+  a.segs = T.segs[kind];
+  a.nseg = (int32_t)L.segs[kind].size();
+  a.ppm_type = p->ppm_type;
+  a.plm_iorder = p->plm_iorder;
+  a.use_flattening = p->use_flattening;
+  a.difmag = p->difmag;
+  a.dt_dev = dt_dev;
+  const int var = kind < K_NSTAGE ? variant_of(p->precision_mode, L.ns, kind) : 0;
+  cudaError_t e = (p->precision_mode == PCG_PREC_FP64)
+                    ? pcg_strict::launch_stage(kind, L.ns, false, a, L.nblocks[kind], var, s)
+                    : pcg_fast::launch_stage(kind, L.ns, single, a, L.nblocks[kind], var, s);
+  if (e != cudaSuccess) return fail(PCG_ECUDA, "stage %d launch: %s", kind, cudaGetErrorString(e));
+  return PCG_OK;
 }
 
 int launch_stages(const Layout& L, const Tables& T, const pcg_hydro_params* p, int first, int last,
                   const double* dt_dev, cudaStream_t s) {
-  const bool single = p->precision_mode == PCG_PREC_MIXED;
   for (int st = first; st <= last; ++st) {
-    if (L.nblocks[st] == 0) continue;
-    pcg::StageArgs a{};
-    a.regions = T.regions;
-    a.segs = T.segs[st];
-    a.nseg = (int32_t)L.segs[st].size();
-    a.ppm_type = p->ppm_type;
-    a.plm_iorder = p->plm_iorder;
-    a.use_flattening = p->use_flattening;
-    a.difmag = p->difmag;
-    a.dt_dev = dt_dev;
-    const int var = variant_of(p->precision_mode, L.ns, st);
-    cudaError_t e = (p->precision_mode == PCG_PREC_FP64)
-                      ? pcg_strict::launch_stage(st, L.ns, false, a, L.nblocks[st], var, s)
-                      : pcg_fast::launch_stage(st, L.ns, single, a, L.nblocks[st], var, s);
-    if (e != cudaSuccess) return fail(PCG_ECUDA, "stage %d launch: %s", st, cudaGetErrorString(e));
+    int rc = launch_kind(L, T, p, st, dt_dev, s);
+    if (rc == PCG_OK && st == K_FLUX2) rc = launch_kind(L, T, p, K_LOWBC, dt_dev, s);
+    if (rc) return rc;
   }
   return PCG_OK;
 }
@@ -1031,6 +1058,7 @@ int pcg_plan_info(const pcg_plan* P, int64_t* workspace_bytes, int32_t* nregions
   if (nregions) *nregions = (int32_t)P->L.regions.size();
   if (blocks_per_stage)
     for (int s = 0; s < K_NSTAGE; ++s) blocks_per_stage[s] = P->L.nblocks[s];
+    blocks_per_stage[K_FLUX2] += P->L.nblocks[K_LOWBC];
   return PCG_OK;
 }
 

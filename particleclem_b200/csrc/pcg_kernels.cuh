@@ -11,6 +11,8 @@
 //   K_FLUX1    pc_transdo + Riemann for both transverse partners of d  -> fdo[d][o]
 //   K_FLUX2    pc_transdd + final Riemann + pc_artif_visc + pc_norm_spec_flx
 //              + pc_ext_flx                                             -> ff[d], qec[d]
+//   K_LOWBC    pc_low_order_boundary: inflow/user_bc domain faces again from
+//              PLM states without transverse terms, after K_FLUX2      -> ff[d], qec[d]
 //   K_CONSUP   pc_pdivu + pc_update                                     -> uout
 // Traced states are kept only for the cells whose states reach the box's fluxes
 // (grow(box,1)); the reference traces grow(box,2), whose outer layer feeds no output.
@@ -24,6 +26,7 @@
 namespace PCG_TU {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
+enum { K_LOWBC = K_NSTAGE };  // inflow/user_bc boundary faces, launched within stage K_FLUX2
 
 // Launch variants: each heavy stage is compiled with a few minimum-resident-blocks
 // requests (__launch_bounds__ register caps); the host picks one per (form, species
@@ -408,10 +411,19 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
   }
 }
 
-// Source/PLM.H:167-309 (pc_plm_d) with the slopes of Source/Godunov.cpp:139-180.
-template <int NS, bool MIX, int D, class R>
-__device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
-                                              double dt) {
+// A traced state held in registers (the low-order boundary faces).
+template <class R>
+struct RegState {
+  R* a;
+  __device__ __forceinline__ R& operator[](int n) const { return a[n]; }
+};
+
+// Source/PLM.H:167-309 (pc_plm_d) with the slopes of Source/Godunov.cpp:139-180, for the
+// cell (i, j, k) and direction D: qp receives the state on the cell's low D-face (the
+// right state of that face), qm the state on its high D-face (the left state there).
+template <int NS, bool MIX, int D, class R, class QP, class QM>
+__device__ __forceinline__ void plm_cell(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
+                                         double dt, const QP& qp, const QM& qm) {
   constexpr int l1 = (D == 0) ? 1 : 0;
   constexpr int l2 = (D == 2) ? 1 : 2;
   const Prim<R> P(rg, i, j, k, D);
@@ -436,8 +448,6 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
   const R alpha0v = dvel[l1];
   const R alpha0w = dvel[l2];
   const R wv[3] = {vel[D] - cc, vel[D], vel[D] + cc};
-  const CellPtr<R> qp = at(v4<R>(rg.trp[D]), i, j, k);
-  const CellPtr<R> qm = at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2));
   {
     const R rho_ref = rho - R(0.5) * (R(1) + dtdx * dmin(wv[0], R(0))) * drho;
     R vel_ref[3];
@@ -495,6 +505,13 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
     qm[pcg::TR_Y + n] = qc + acmpleft;
   }
 #undef SLOPE
+}
+
+template <int NS, bool MIX, int D, class R>
+__device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
+                                              double dt) {
+  plm_cell<NS, MIX, D, R>(rg, i, j, k, cc, flat, order, dt, at(v4<R>(rg.trp[D]), i, j, k),
+                          at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2)));
 }
 
 template <int NS, bool MIX, bool EXACT, int D, class R>
@@ -1147,6 +1164,39 @@ __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
     case 0: flux2_x<NS, MIX, EXACT, R>(a, sg, t, kcarry); break;
     case 1: flux2_march<NS, MIX, EXACT, 1, R>(a, sg, t, kcarry); break;
     default: flux2_march<NS, MIX, EXACT, 2, R>(a, sg, t, kcarry); break;
+  }
+}
+
+// Source/Godunov.cpp:6-55 (pc_low_order_boundary), called at :440-468 for the faces of a
+// box on an inflow or user_bc domain boundary: the boundary state is given at time n, so
+// the final flux there comes from PLM states of the two adjacent cells (slopes with the
+// cell's flattening, the cell's qaux sound speed) without transverse corrections; the
+// flux adjustments of pc_adjust_fluxes follow as for every face. Runs after K_FLUX2 and
+// overwrites its results on those faces.
+template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void lowbc_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+  const int di = (D == 0), dj = (D == 1), dk = (D == 2);
+  const double dt = dt_of(a, rg);
+  const V4<const double> qav = v4<const double>(rg.qa);
+  const V4<const R> prv = v4<const R>(rg.prep);
+  R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)], unused[pcg::nt_comps(NS)];
+  // left state: the high-side state of the cell behind the face
+  plm_cell<NS, MIX, D, R>(rg, i - di, j - dj, k - dk, R(qav(i - di, j - dj, k - dk, pcg::QC)),
+                          prv(i - di, j - dj, k - dk, 0), a.plm_iorder, dt, RegState<R>{unused}, RegState<R>{ql});
+  // right state: the low-side state of the face's own cell
+  plm_cell<NS, MIX, D, R>(rg, i, j, k, R(qav(i, j, k, pcg::QC)), prv(i, j, k, 0), a.plm_iorder, dt,
+                          RegState<R>{qr}, RegState<R>{unused});
+  flux2_face<NS, MIX, EXACT, D, R>(a, rg, i, j, k, ql, qr, p0_of<NS, MIX, R>(rg));
+}
+
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_lowbc(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  switch (it.variant) {
+    case 0: lowbc_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: lowbc_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+    default: lowbc_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
   }
 }
 

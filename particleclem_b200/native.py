@@ -86,8 +86,8 @@ def header_functions(path: str = HEADER):
 
 
 def lib_path() -> str:
-    """The library to load: PCG_LIB if set (an alternative build, e.g. from the
-    launch-shape tuner), else the in-tree build."""
+    """The library to load: PCG_LIB if set (an alternative build), else the in-tree
+    build."""
     from .build import LIB
     return os.environ.get("PCG_LIB", LIB)
 

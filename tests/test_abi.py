@@ -41,8 +41,10 @@ def test_argument_errors_are_codes_not_aborts():
     assert _rc("pcg_plan_destroy", None) == 0
 
 
-@pytest.mark.parametrize("bc", [abi.BC_INFLOW, abi.BC_USER])
-def test_inflow_boundaries_are_reported_unsupported(bc):
+@pytest.mark.parametrize("bc", [-1, 7])
+def test_unknown_boundary_types_are_rejected(bc):
+    """Boundary codes outside PeleC's PCPhysBCType (Source/PeleC.H:49-57) fail with
+    PCG_EINVAL before any device work; inflow and user_bc are accepted (low-order faces)."""
     import numpy as np
 
     prm = abi.make_params((1, 1, 1), 0.1, 1, (0, 0, 0), (7, 7, 7), (bc, 0, 0), (0, 0, 0))
@@ -50,4 +52,4 @@ def test_inflow_boundaries_are_reported_unsupported(bc):
     o = abi.Fab(np.zeros((8, 8, 8, 8)), (0, 0, 0))
     rc = _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), C.byref(abi.array4(u)),
              C.byref(abi.array4(o)), None, None)
-    assert rc == -4
+    assert rc == -1

@@ -35,7 +35,7 @@ enum {
   PCG_EINVAL = -1,       /* bad argument (box, array extent, parameter) */
   PCG_ECUDA = -2,        /* a CUDA runtime call failed */
   PCG_ENOMEM = -3,       /* device allocation failed */
-  PCG_EUNSUPPORTED = -4, /* option not implemented (hybrid WENO, nspec other than 1 or 9) */
+  PCG_EUNSUPPORTED = -4, /* option not implemented (nspec other than 1 or 9) */
   PCG_ETIMEDOUT = -5,    /* a bounded device wait gave up */
   PCG_EBUDGET = -6,      /* serving: request exceeds the memory budget */
   PCG_ENOEOS = -7        /* no EOS table set for this species count */

@@ -438,10 +438,113 @@ static void ppm_int_profile(double sm, double sp, double sc, double u, double c,
   }
 }
 
+/* Source/WENO.H: the hybrid-WENO edge values of cell s[c] (sm on its low face, sp on its
+ * high face) that replace the PPM parabola in trace_ppm when use_hybrid_weno is set
+ * (Source/PPM.cpp:120-172). Published schemes: WENO-JS5 (Jiang & Shu 1996), WENO-Z5
+ * (Borges et al. 2008), WENO-Z7 (Balsara & Shu 2000 stencils with Z weights), WENO-Z3;
+ * every expression keeps the reference's order of operations (pow(x, 2) is x * x). */
+static const double WENO_EPS = 1e-6;
+static inline double sq(double x) { return x * x; }
+
+/* smoothness of the three 3-point substencils of a 5-point stencil seen from the high
+ * face, and mirrored from the low face */
+static void w5_beta_hi(const double* s, double* b) {
+  b[2] = (13.0 / 12.0) * sq(s[0] - 2.0 * s[1] + s[2]) + 0.25 * sq(s[0] - 4.0 * s[1] + 3.0 * s[2]);
+  b[1] = (13.0 / 12.0) * sq(s[1] - 2.0 * s[2] + s[3]) + 0.25 * (s[1] - s[3]) * (s[1] - s[3]);
+  b[0] = (13.0 / 12.0) * sq(s[2] - 2.0 * s[3] + s[4]) + 0.25 * sq(3.0 * s[2] - 4.0 * s[3] + s[4]);
+}
+static void w5_beta_lo(const double* s, double* b) {
+  b[2] = (13.0 / 12.0) * sq(s[4] - 2.0 * s[3] + s[2]) + 0.25 * sq(s[4] - 4.0 * s[3] + 3.0 * s[2]);
+  b[1] = (13.0 / 12.0) * sq(s[3] - 2.0 * s[2] + s[1]) + 0.25 * (s[3] - s[1]) * (s[3] - s[1]);
+  b[0] = (13.0 / 12.0) * sq(s[2] - 2.0 * s[1] + s[0]) + 0.25 * sq(3.0 * s[2] - 4.0 * s[1] + s[0]);
+}
+/* nonlinear weights from the smoothness indicators, in place: JS 1/(eps+b)^2, Z 1+(tau/(eps+b))^2 */
+static void w_weights(double* b, int n, double tau, int z) {
+  for (int m = 0; m < n; ++m)
+    b[m] = z ? 1.0 + (tau / (WENO_EPS + b[m])) * (tau / (WENO_EPS + b[m]))
+             : 1.0 / ((WENO_EPS + b[m]) * (WENO_EPS + b[m]));
+}
+static double w5_blend(const double* b, const double* v) {
+  const double a2 = b[2], a1 = 6.0 * b[1], a0 = 3.0 * b[0];
+  const double ai = 1.0 / (a2 + a1 + a0);
+  return (1.0 / 6.0) * ai * (a2 * v[2] + a1 * v[1] + a0 * v[0]);
+}
+static void weno5(const double* s, int z, double* sm, double* sp) {
+  double b[3], v[3];
+  w5_beta_hi(s, b);
+  w_weights(b, 3, fabs(b[2] - b[0]), z);
+  v[2] = 2.0 * s[0] - 7.0 * s[1] + 11.0 * s[2];
+  v[1] = -s[1] + 5.0 * s[2] + 2.0 * s[3];
+  v[0] = 2.0 * s[2] + 5.0 * s[3] - s[4];
+  *sp = w5_blend(b, v);
+  w5_beta_lo(s, b);
+  w_weights(b, 3, fabs(b[2] - b[0]), z);
+  v[2] = 11.0 * s[2] - 7.0 * s[3] + 2.0 * s[4];
+  v[1] = -s[3] + 5.0 * s[2] + 2.0 * s[1];
+  v[0] = 2.0 * s[2] + 5.0 * s[1] - s[0];
+  *sm = w5_blend(b, v);
+}
+/* smoothness polynomial of the 4-point substencil (a, b, c, d) of WENO-7 with the
+ * coefficient set k (the same shape for all four substencils) */
+static double w7_beta(double a, double b, double c, double d, const double* k) {
+  return a * (k[0] * a - k[1] * b + k[2] * c - k[3] * d) + b * (k[4] * b - k[5] * c + k[6] * d) +
+         c * (k[7] * c - k[8] * d) + k[9] * (d * d);
+}
+static const double W7K[4][10] = {
+  {2107.0, 9402.0, 7042.0, 1854.0, 11003.0, 17246.0, 4642.0, 7043.0, 3882.0, 547.0},
+  {547.0, 2522.0, 1922.0, 494.0, 3443.0, 5966.0, 1602.0, 2843.0, 1642.0, 267.0},
+  {267.0, 1642.0, 1602.0, 494.0, 2843.0, 5966.0, 1922.0, 3443.0, 2522.0, 547.0},
+  {547.0, 3882.0, 4642.0, 1854.0, 7043.0, 17246.0, 7042.0, 11003.0, 9402.0, 2107.0},
+};
+static double w7_blend(const double* b, const double* v) {
+  const double a3 = (1.0 / 35.0) * b[3], a2 = (12.0 / 35.0) * b[2], a1 = (18.0 / 35.0) * b[1],
+               a0 = (4.0 / 35.0) * b[0];
+  const double ai = 1.0 / (a3 + a2 + a1 + a0);
+  return (1.0 / 12.0) * ai * (a3 * v[3] + a2 * v[2] + a1 * v[1] + a0 * v[0]);
+}
+static void weno7z(const double* s, double* sm, double* sp) {
+  double b[4], v[4];
+  b[3] = w7_beta(s[0], s[1], s[2], s[3], W7K[3]);
+  b[2] = w7_beta(s[1], s[2], s[3], s[4], W7K[2]);
+  b[1] = w7_beta(s[2], s[3], s[4], s[5], W7K[1]);
+  b[0] = w7_beta(s[3], s[4], s[5], s[6], W7K[0]);
+  w_weights(b, 4, fabs(b[3] - b[0]), 1);
+  v[3] = -3.0 * s[0] + 13.0 * s[1] - 23.0 * s[2] + 25.0 * s[3];
+  v[2] = s[1] - 5.0 * s[2] + 13.0 * s[3] + 3.0 * s[4];
+  v[1] = -s[2] + 7.0 * s[3] + 7.0 * s[4] - s[5];
+  v[0] = 3.0 * s[3] + 13.0 * s[4] - 5.0 * s[5] + s[6];
+  *sp = w7_blend(b, v);
+  b[3] = w7_beta(s[6], s[5], s[4], s[3], W7K[3]);
+  b[2] = w7_beta(s[5], s[4], s[3], s[2], W7K[2]);
+  b[1] = w7_beta(s[4], s[3], s[2], s[1], W7K[1]);
+  b[0] = w7_beta(s[3], s[2], s[1], s[0], W7K[0]);
+  w_weights(b, 4, fabs(b[3] - b[0]), 1);
+  v[3] = -3.0 * s[6] + 13.0 * s[5] - 23.0 * s[4] + 25.0 * s[3];
+  v[2] = s[5] - 5.0 * s[4] + 13.0 * s[3] + 3.0 * s[2];
+  v[1] = -s[4] + 7.0 * s[3] + 7.0 * s[2] - s[1];
+  v[0] = 3.0 * s[3] + 13.0 * s[2] - 5.0 * s[1] + s[0];
+  *sm = w7_blend(b, v);
+}
+static void weno3z(const double* s, double* sm, double* sp) {
+  double b[2];
+  b[1] = (s[0] - s[1]) * (s[0] - s[1]);
+  b[0] = (s[1] - s[2]) * (s[1] - s[2]);
+  w_weights(b, 2, fabs(b[1] - b[0]), 1);
+  double a1 = 2.0 * b[1], a0 = 1.0 * b[0], ai = 1.0 / (a1 + a0);
+  *sp = 0.5 * ai * (a1 * (-s[0] + 3.0 * s[1]) + a0 * (s[1] + s[2]));
+  b[1] = (s[2] - s[1]) * (s[2] - s[1]);
+  b[0] = (s[1] - s[0]) * (s[1] - s[0]);
+  w_weights(b, 2, fabs(b[1] - b[0]), 1);
+  a1 = 2.0 * b[1];
+  a0 = 1.0 * b[0];
+  ai = 1.0 / (a1 + a0);
+  *sm = 0.5 * ai * (a1 * (3.0 * s[1] - s[2]) + a0 * (s[0] + s[1]));
+}
+
 /* Source/PPM.cpp:6-424 (trace_ppm, ORIGINAL PPM branch; bx == vbx as called from
  * Godunov.cpp:188-200, so both face states are written for every cell). */
 static void trace_ppm(box_t bx, int idir, const fab_t* q, fab_t* qm, fab_t* qp, double dt,
-                      const double* dx, int use_flattening) {
+                      const double* dx, int use_flattening, int use_hybrid_weno, int weno_scheme) {
   const double dtdx = dt / dx[idir];
   const int QUN = (idir == 0) ? QU : (idir == 1) ? QV : QW;
   const int QUT = (idir == 0) ? QV : (idir == 1) ? QW : QU;
@@ -460,12 +563,29 @@ static void trace_ppm(box_t bx, int idir, const fab_t* q, fab_t* qm, fab_t* qp, 
     }
     double Ip[MAXQ][3], Im[MAXQ][3];
     for (int n = 0; n < QVAR; n++) {
-      double s[5];
-      for (int o = -2; o <= 2; ++o)
-        s[o + 2] = F(*q, i + o * dv[0], j + o * dv[1], k + o * dv[2], n);
-      double sm, sp;
-      ppm_reconstruct(s, flat, &sm, &sp);
-      ppm_int_profile(sm, sp, s[2], un, cc, dtdx, Ip[n], Im[n]);
+      double s[7], sm, sp;
+      if (use_hybrid_weno && weno_scheme == 2) {
+        /* on the outer ring of bx the stencil leaves q's grow(bx,4) box (the reference reads
+         * beyond its allocation there); those traces feed no output, the read is clamped */
+        for (int o = -3; o <= 3; ++o) {
+          int c[3] = {i + o * dv[0], j + o * dv[1], k + o * dv[2]};
+          for (int e = 0; e < 3; ++e) c[e] = c[e] < q->lo[e] ? q->lo[e] : c[e] > q->hi[e] ? q->hi[e] : c[e];
+          s[o + 3] = F(*q, c[0], c[1], c[2], n);
+        }
+        weno7z(s, &sm, &sp);
+        ppm_int_profile(sm, sp, s[3], un, cc, dtdx, Ip[n], Im[n]);
+      } else if (use_hybrid_weno && weno_scheme == 3) {
+        for (int o = -1; o <= 1; ++o) s[o + 1] = F(*q, i + o * dv[0], j + o * dv[1], k + o * dv[2], n);
+        weno3z(s, &sm, &sp);
+        ppm_int_profile(sm, sp, s[1], un, cc, dtdx, Ip[n], Im[n]);
+      } else {
+        for (int o = -2; o <= 2; ++o) s[o + 2] = F(*q, i + o * dv[0], j + o * dv[1], k + o * dv[2], n);
+        if (use_hybrid_weno && (weno_scheme == 0 || weno_scheme == 1))
+          weno5(s, weno_scheme == 1, &sm, &sp);
+        else
+          ppm_reconstruct(s, flat, &sm, &sp);
+        ppm_int_profile(sm, sp, s[2], un, cc, dtdx, Ip[n], Im[n]);
+      }
     }
     for (int n = QFS; n < g_ns + QFS; n++) {
       F(*qp, i, j, k, n) = Im[n][1];
@@ -1076,7 +1196,7 @@ static void low_order_boundary(box_t bfbx, int bclo, int bchi, int domlo, int do
 static int umeth_3d(box_t bx, const int* bclo, const int* bchi, const int* domlo, const int* domhi,
                     const fab_t* q, const fab_t* qaux, const fab_t* srcQ, fab_t* flx, fab_t* qec,
                     const fab_t* a, fab_t* pdivu, const fab_t* vol, const double* del, double dt,
-                    int ppm_type, int plm_iorder, int use_flattening) {
+                    int ppm_type, int plm_iorder, int use_flattening, int use_hybrid_weno, int weno_scheme) {
   const double dx = del[0], dy = del[1], dz = del[2];
   const double hdtdx = 0.5 * dt / dx, hdtdy = 0.5 * dt / dy, hdtdz = 0.5 * dt / dz;
   const double cdtdx = 1.0 / 3.0 * dt / dx, cdtdy = 1.0 / 3.0 * dt / dy, cdtdz = 1.0 / 3.0 * dt / dz;
@@ -1101,7 +1221,8 @@ static int umeth_3d(box_t bx, const int* bclo, const int* bchi, const int* domlo
       }
     }
   } else if (ppm_type == 1) {
-    for (int d = 0; d < 3; ++d) trace_ppm(bxg2, d, q, &qdm[d], &qdp[d], dt, del, use_flattening);
+    for (int d = 0; d < 3; ++d)
+      trace_ppm(bxg2, d, q, &qdm[d], &qdp[d], dt, del, use_flattening, use_hybrid_weno, weno_scheme);
   } else {
     for (int d = 0; d < 3; ++d) { fab_free(&qdm[d]); fab_free(&qdp[d]); }
     return -2;
@@ -1210,7 +1331,8 @@ int orc_umdrv(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], c
   fab_t vf = fab_view(vol);
   fab_t divu = fab_new(bxg2, 1), pdivu = fab_new(bx, 1);
   int rc = umeth_3d(bx, prm->bclo, prm->bchi, prm->domlo, prm->domhi, &qf, &af, sfp, ff, qec, aa, &pdivu,
-                    &vf, prm->dx, prm->dt, prm->ppm_type, prm->plm_iorder, prm->use_flattening);
+                    &vf, prm->dx, prm->dt, prm->ppm_type, prm->plm_iorder, prm->use_flattening,
+                    prm->use_hybrid_weno, prm->weno_scheme);
   if (rc == 0) {
     const double dx = prm->dx[0], dy = prm->dx[1], dz = prm->dx[2];
     FOR_BOX(bxg2, i, j, k) {

@@ -119,7 +119,12 @@ int ref_hydro_box(const orc_params* prm, const int32_t lo[3], const int32_t hi[3
   if (prm->nspec != NUM_SPECIES) return -3;
   const amrex::Box bx = mkbox(lo, hi);
   const amrex::Box qbx = grow(bx, 4);
-  amrex::FArrayBox q(qbx, QVAR), qaux(qbx, NQAUX), src_q(qbx, QVAR), src_in(qbx, NVAR);
+  // q, qaux and src_q carry one more ring than the reference allocates: its WENO-Z7 trace
+  // (use_hybrid_weno, weno_scheme 2) reads q one cell beyond grow(bx,4) on the outer ring
+  // of its traced box, whose states feed no output. The ring holds copies of the nearest
+  // computed cell, so that read stays inside the allocation.
+  const amrex::Box qbx5 = grow(bx, 5);
+  amrex::FArrayBox q(qbx5, QVAR), qaux(qbx5, NQAUX), src_q(qbx5, QVAR), src_in(qbx5, NVAR);
   auto const& qarr = q.array();
   auto const& qauxar = qaux.array();
   auto const& srcqarr = src_q.array();
@@ -127,6 +132,18 @@ int ref_hydro_box(const orc_params* prm, const int32_t lo[3], const int32_t hi[3
   amrex::Array4<const amrex::Real> srcin = src_in.const_array();
   amrex::ParallelFor(qbx, [=](int i, int j, int k) { pc_ctoprim(i, j, k, sarr, qarr, qauxar); });
   amrex::ParallelFor(qbx, [=](int i, int j, int k) { pc_srctoprim(i, j, k, qarr, qauxar, srcin, srcqarr); });
+  {
+    const auto l = qbx.loVect3d();
+    const auto h = qbx.hiVect3d();
+    amrex::ParallelFor(qbx5, [=](int i, int j, int k) {
+      const int ci = std::min(std::max(i, l[0]), h[0]), cj = std::min(std::max(j, l[1]), h[1]),
+                ck = std::min(std::max(k, l[2]), h[2]);
+      if (ci == i && cj == j && ck == k) return;
+      for (int n = 0; n < QVAR; ++n) qarr(i, j, k, n) = qarr(ci, cj, ck, n);
+      for (int n = 0; n < NQAUX; ++n) qauxar(i, j, k, n) = qauxar(ci, cj, ck, n);
+      for (int n = 0; n < QVAR; ++n) srcqarr(i, j, k, n) = srcqarr(ci, cj, ck, n);
+    });
+  }
   auto hyd_src = view(uout);
   amrex::ParallelFor(bx, [=](int i, int j, int k) {
     for (int n = 0; n < NVAR; ++n) hyd_src(i, j, k, n) = 0.0;

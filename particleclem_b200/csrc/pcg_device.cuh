@@ -35,6 +35,13 @@ template <> struct Lim<float> {
 template <class R> __device__ __forceinline__ R dmin(R a, R b) { return (b < a) ? b : a; }
 template <class R> __device__ __forceinline__ R dmax(R a, R b) { return (a < b) ? b : a; }
 
+// The reference's clamps to [0, 1], nested std::min/std::max, including their results
+// for NaN: max(0, min(1, NaN)) is 1 and min(1, max(0, NaN)) is 0. The NaN case is
+// written out because the device compiler folds a nested min/max into a saturating
+// clamp, which maps NaN to 0 in both orders.
+template <class R> __device__ __forceinline__ R max0_min1(R x) { return (x != x) ? R(1) : dmax(R(0), dmin(R(1), x)); }
+template <class R> __device__ __forceinline__ R min1_max0(R x) { return (x != x) ? R(0) : dmin(R(1), dmax(R(0), x)); }
+
 // Pressure in the FP32 arithmetic is carried as the deviation p' = p - p0 from a
 // constant p0 of the box (rho*R/W*T of its first cell): PPM/PLM reconstruction, the
 // characteristic projection, the linearised star state and the flux differences are
@@ -294,6 +301,112 @@ struct EosR {
   }
 };
 
+// ------------------------------------------------------------------ hybrid WENO
+// Source/WENO.H: edge values of the centre cell of a stencil (sm on its low face, sp on
+// its high face) replacing the PPM parabola when use_hybrid_weno is set
+// (Source/PPM.cpp:120-172): WENO-JS5 (Jiang & Shu 1996), WENO-Z5 (Borges et al. 2008),
+// WENO-Z7 (Balsara & Shu 2000 stencils, Z weights), WENO-Z3. Each expression keeps the
+// reference's operation order (pow(x, 2) is x * x), so the FP64 form is bit-identical.
+namespace weno {
+template <class R> __device__ __forceinline__ R sq(R x) { return x * x; }
+template <class R> __device__ __forceinline__ R eps() { return R(1e-6); }
+
+template <class R>
+__device__ __forceinline__ void w_weights(R* b, int n, R tau, bool z) {
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    if (m < n)
+      b[m] = z ? R(1) + (tau / (eps<R>() + b[m])) * (tau / (eps<R>() + b[m]))
+               : R(1) / ((eps<R>() + b[m]) * (eps<R>() + b[m]));
+}
+template <class R>
+__device__ __forceinline__ R w5_blend(const R* b, const R* v) {
+  const R a2 = b[2], a1 = R(6) * b[1], a0 = R(3) * b[0];
+  const R ai = R(1) / (a2 + a1 + a0);
+  return R(1.0 / 6.0) * ai * (a2 * v[2] + a1 * v[1] + a0 * v[0]);
+}
+template <class R>
+__device__ __forceinline__ void weno5(const R* s, bool z, R& sm, R& sp) {
+  const R k13 = R(13.0 / 12.0);
+  R b[3], v[3];
+  b[2] = k13 * sq(s[0] - R(2) * s[1] + s[2]) + R(0.25) * sq(s[0] - R(4) * s[1] + R(3) * s[2]);
+  b[1] = k13 * sq(s[1] - R(2) * s[2] + s[3]) + R(0.25) * (s[1] - s[3]) * (s[1] - s[3]);
+  b[0] = k13 * sq(s[2] - R(2) * s[3] + s[4]) + R(0.25) * sq(R(3) * s[2] - R(4) * s[3] + s[4]);
+  w_weights(b, 3, fabs(b[2] - b[0]), z);
+  v[2] = R(2) * s[0] - R(7) * s[1] + R(11) * s[2];
+  v[1] = -s[1] + R(5) * s[2] + R(2) * s[3];
+  v[0] = R(2) * s[2] + R(5) * s[3] - s[4];
+  sp = w5_blend(b, v);
+  b[2] = k13 * sq(s[4] - R(2) * s[3] + s[2]) + R(0.25) * sq(s[4] - R(4) * s[3] + R(3) * s[2]);
+  b[1] = k13 * sq(s[3] - R(2) * s[2] + s[1]) + R(0.25) * (s[3] - s[1]) * (s[3] - s[1]);
+  b[0] = k13 * sq(s[2] - R(2) * s[1] + s[0]) + R(0.25) * sq(R(3) * s[2] - R(4) * s[1] + s[0]);
+  w_weights(b, 3, fabs(b[2] - b[0]), z);
+  v[2] = R(11) * s[2] - R(7) * s[3] + R(2) * s[4];
+  v[1] = -s[3] + R(5) * s[2] + R(2) * s[1];
+  v[0] = R(2) * s[2] + R(5) * s[1] - s[0];
+  sm = w5_blend(b, v);
+}
+// smoothness of the 4-point substencil (a, b, c, d) of WENO-7 with coefficient set K
+template <class R, int K>
+__device__ __forceinline__ R w7_beta(R a, R b, R c, R d) {
+  constexpr double k[4][10] = {
+    {2107.0, 9402.0, 7042.0, 1854.0, 11003.0, 17246.0, 4642.0, 7043.0, 3882.0, 547.0},
+    {547.0, 2522.0, 1922.0, 494.0, 3443.0, 5966.0, 1602.0, 2843.0, 1642.0, 267.0},
+    {267.0, 1642.0, 1602.0, 494.0, 2843.0, 5966.0, 1922.0, 3443.0, 2522.0, 547.0},
+    {547.0, 3882.0, 4642.0, 1854.0, 7043.0, 17246.0, 7042.0, 11003.0, 9402.0, 2107.0}};
+  return a * (R(k[K][0]) * a - R(k[K][1]) * b + R(k[K][2]) * c - R(k[K][3]) * d) +
+         b * (R(k[K][4]) * b - R(k[K][5]) * c + R(k[K][6]) * d) + c * (R(k[K][7]) * c - R(k[K][8]) * d) +
+         R(k[K][9]) * (d * d);
+}
+template <class R>
+__device__ __forceinline__ R w7_blend(const R* b, const R* v) {
+  const R a3 = R(1.0 / 35.0) * b[3], a2 = R(12.0 / 35.0) * b[2], a1 = R(18.0 / 35.0) * b[1],
+          a0 = R(4.0 / 35.0) * b[0];
+  const R ai = R(1) / (a3 + a2 + a1 + a0);
+  return R(1.0 / 12.0) * ai * (a3 * v[3] + a2 * v[2] + a1 * v[1] + a0 * v[0]);
+}
+template <class R>
+__device__ __forceinline__ void weno7z(const R* s, R& sm, R& sp) {
+  R b[4], v[4];
+  b[3] = w7_beta<R, 3>(s[0], s[1], s[2], s[3]);
+  b[2] = w7_beta<R, 2>(s[1], s[2], s[3], s[4]);
+  b[1] = w7_beta<R, 1>(s[2], s[3], s[4], s[5]);
+  b[0] = w7_beta<R, 0>(s[3], s[4], s[5], s[6]);
+  w_weights(b, 4, fabs(b[3] - b[0]), true);
+  v[3] = R(-3) * s[0] + R(13) * s[1] - R(23) * s[2] + R(25) * s[3];
+  v[2] = s[1] - R(5) * s[2] + R(13) * s[3] + R(3) * s[4];
+  v[1] = -s[2] + R(7) * s[3] + R(7) * s[4] - s[5];
+  v[0] = R(3) * s[3] + R(13) * s[4] - R(5) * s[5] + s[6];
+  sp = w7_blend(b, v);
+  b[3] = w7_beta<R, 3>(s[6], s[5], s[4], s[3]);
+  b[2] = w7_beta<R, 2>(s[5], s[4], s[3], s[2]);
+  b[1] = w7_beta<R, 1>(s[4], s[3], s[2], s[1]);
+  b[0] = w7_beta<R, 0>(s[3], s[2], s[1], s[0]);
+  w_weights(b, 4, fabs(b[3] - b[0]), true);
+  v[3] = R(-3) * s[6] + R(13) * s[5] - R(23) * s[4] + R(25) * s[3];
+  v[2] = s[5] - R(5) * s[4] + R(13) * s[3] + R(3) * s[2];
+  v[1] = -s[4] + R(7) * s[3] + R(7) * s[2] - s[1];
+  v[0] = R(3) * s[3] + R(13) * s[2] - R(5) * s[1] + s[0];
+  sm = w7_blend(b, v);
+}
+template <class R>
+__device__ __forceinline__ void weno3z(const R* s, R& sm, R& sp) {
+  R b[2];
+  b[1] = (s[0] - s[1]) * (s[0] - s[1]);
+  b[0] = (s[1] - s[2]) * (s[1] - s[2]);
+  w_weights(b, 2, fabs(b[1] - b[0]), true);
+  R a1 = R(2) * b[1], a0 = R(1) * b[0], ai = R(1) / (a1 + a0);
+  sp = R(0.5) * ai * (a1 * (-s[0] + R(3) * s[1]) + a0 * (s[1] + s[2]));
+  b[1] = (s[2] - s[1]) * (s[2] - s[1]);
+  b[0] = (s[1] - s[0]) * (s[1] - s[0]);
+  w_weights(b, 2, fabs(b[1] - b[0]), true);
+  a1 = R(2) * b[1];
+  a0 = R(1) * b[0];
+  ai = R(1) / (a1 + a0);
+  sm = R(0.5) * ai * (a1 * (R(3) * s[1] - s[2]) + a0 * (s[0] + s[1]));
+}
+}  // namespace weno
+
 // ------------------------------------------------------------------ PPM
 // Source/PPM.H:28-115 (ppm_reconstruct)
 template <class R>
@@ -376,7 +489,7 @@ __device__ __forceinline__ R flatten(const V4<const double>& q, int i, int j, in
   const int ishft = (dp > R(0)) ? 1 : -1;
   R denom = dmax(small_pres, fabs(qpp - qmm));
   R zeta = fabs(dp) / denom;
-  const R z = dmin(R(1), dmax(R(0), dzcut * (zeta - zcut1)));
+  const R z = min1_max0<R>(dzcut * (zeta - zcut1));
   R tst = (qmun - qpun >= R(0)) ? R(1) : R(0);
   R tmp = dmin(qp, qm);
   const R chi = (fabs(dp) / tmp) > shktst ? tst : R(0);
@@ -389,7 +502,7 @@ __device__ __forceinline__ R flatten(const V4<const double>& q, int i, int j, in
   dp = qpshft - qmshft;
   denom = dmax(small_pres, fabs(qppshft - qmmshft));
   zeta = fabs(dp) / denom;
-  const R z2 = dmin(R(1), dmax(R(0), dzcut * (zeta - zcut1)));
+  const R z2 = min1_max0<R>(dzcut * (zeta - zcut1));
   tst = (qmunshft - qpunshft >= R(0)) ? R(1) : R(0);
   tmp = dmin(qpshft, qmshft);
   const R chi2 = (fabs(dp) / tmp) > shktst ? tst : R(0);
@@ -491,7 +604,7 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
   spout = mask ? spout : ushock;
   spin = mask ? spin : ushock;
   const R scr = (fabs(spout - spin) < Lim<R>::very_small()) ? R(pcg::SMALL_NUM) * cav : spout - spin;
-  const R frac = dmax(R(0), dmin(R(1), (R(1) + rdiv(spout + spin, scr)) * R(0.5)));
+  const R frac = max0_min1<R>((R(1) + rdiv(spout + spin, scr)) * R(0.5));
   mask = ustar > R(0);
   R qint_iv1 = mask ? vl : vr;
   R qint_iv2 = mask ? v2l : v2r;
@@ -584,7 +697,7 @@ __device__ __forceinline__ void riemann(const FaceState<NS, R>& L, const FaceSta
   spout = mask ? spout : ushock;
   spin = mask ? spin : ushock;
   const R scr = (fabs(spout - spin) < Lim<R>::very_small()) ? R(pcg::SMALL_NUM) * cav : spout - spin;
-  const R frac = dmax(R(0), dmin(R(1), (R(1) + (spout + spin) / scr) * R(0.5)));
+  const R frac = max0_min1<R>((R(1) + (spout + spin) / scr) * R(0.5));
 
   mask = ustar > R(0);
   R qint_iv1 = mask ? vl : vr;

@@ -26,14 +26,17 @@ static cudaError_t launch_v(int stage, const pcg::StageArgs& a, const dim3& grid
   switch (stage) {
     case K_CTOPRIM: k_ctoprim<NS, MIX, kMinBlocks[K_CTOPRIM][V]><<<grid, block, 0, s>>>(a); break;
     case K_PREP: k_prep<NS, MIX, kExact, R><<<grid, block, 0, s>>>(a); break;
-    case K_TRACE: k_trace<NS, MIX, kExact, R, kMinBlocks[K_TRACE][V]><<<grid, block, 0, s>>>(a); break;
+    case K_TRACE:
+      if (a.use_hybrid_weno && a.ppm_type == 1)
+        k_trace_weno<NS, MIX, kExact, R><<<grid, block, 0, s>>>(a);  // one shape for every variant
+      else
+        k_trace<NS, MIX, kExact, R, kMinBlocks[K_TRACE][V]><<<grid, block, 0, s>>>(a);
+      break;
     case K_FLUX0: k_flux0<NS, MIX, kExact, R, kMinBlocks[K_FLUX0][V]><<<grid, block, 0, s>>>(a); break;
     case K_FLUX1: k_flux1<NS, MIX, kExact, R, kMinBlocks[K_FLUX1][V]><<<grid, block, 0, s>>>(a); break;
     case K_FLUX2: k_flux2<NS, MIX, kExact, R, kMinBlocks[K_FLUX2][V]><<<grid, block, 0, s>>>(a); break;
     case K_CONSUP: k_consup<NS, MIX><<<grid, block, 0, s>>>(a); break;
-    case K_LOWBC:
-      if (V == 0) k_lowbc<NS, MIX, kExact, R><<<grid, block, 0, s>>>(a);
-      break;
+    case K_LOWBC: k_lowbc<NS, MIX, kExact, R><<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -211,7 +211,8 @@ int check_params(const pcg_hydro_params* p) {
   if (!p) return fail(PCG_EINVAL, "params is NULL");
   if (p->nspec != 1 && p->nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d: kernels exist for 1 and 9", p->nspec);
   if (p->ppm_type != 0 && p->ppm_type != 1) return fail(PCG_EINVAL, "PeleC::ppm_type must be 0 (PLM) or 1 (PPM)");
-  if (p->use_hybrid_weno) return fail(PCG_EUNSUPPORTED, "hybrid WENO reconstruction is not implemented");
+  if (p->use_hybrid_weno && p->ppm_type != 1)
+    return fail(PCG_EINVAL, "PeleC::ppm_type must be 1 (PPM) to use WENO method");
   if (p->ppm_type == 0 && p->plm_iorder != 1 && p->plm_iorder != 2 && p->plm_iorder != 4)
     return fail(PCG_EINVAL, "plm_iorder must be 1, 2 or 4");
   if (p->precision_mode < PCG_PREC_FP64 || p->precision_mode > PCG_PREC_MIXED)
@@ -273,7 +274,11 @@ void add_seg(Layout& L, int stage, int region, int variant, const IBox& b) {
   L.nblocks[stage] += tiled ? pcg::face_tiles(variant, s.n) : (s.count + kThreads - 1) / kThreads;
 }
 
-void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool single) {
+void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_params* prm) {
+  const int ns = prm->nspec;
+  const bool single = prm->precision_mode == PCG_PREC_MIXED;
+  // the 7-point WENO trace of a cell of grow(box,1) reads primitives on grow(box,4)
+  const int qf_grow = (prm->use_hybrid_weno && prm->ppm_type == 1 && prm->weno_scheme == 2) ? 4 : 3;
   L.ns = ns;
   L.esz = single ? 4 : 8;
   const int nt = pcg::nt_comps(ns), nf = pcg::nf_comps(ns), nv = pcg::nvar(ns), nq = pcg::qvar(ns);
@@ -313,9 +318,10 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, int ns, bool singl
     if (single) {
       // mixed form: the FP32 primitive copy the trace reads, written by k_ctoprim, or by
       // k_prep when the caller supplies q (pcg_umdrv)
-      take(L, grow(B.bx, 3), nt, 4, R.qf);
+      take(L, grow(B.bx, qf_grow), nt, 4, R.qf);
+      R.qf_grow = qf_grow;
       R.qf_in_prep = B.internal_q ? 0 : 1;
-      add_seg(L, K_PREP, (int)r, 0, B.internal_q ? g1 : grow(B.bx, 3));
+      add_seg(L, K_PREP, (int)r, 0, B.internal_q ? g1 : grow(B.bx, qf_grow));
     } else {
       add_seg(L, K_PREP, (int)r, 0, g1);
     }
@@ -444,6 +450,8 @@ int launch_kind(const Layout& L, const Tables& T, const pcg_hydro_params* p, int
   a.ppm_type = p->ppm_type;
   a.plm_iorder = p->plm_iorder;
   a.use_flattening = p->use_flattening;
+  a.use_hybrid_weno = p->use_hybrid_weno;
+  a.weno_scheme = p->weno_scheme;
   a.difmag = p->difmag;
   a.dt_dev = dt_dev;
   const int var = kind < K_NSTAGE ? variant_of(p->precision_mode, L.ns, kind) : 0;
@@ -469,7 +477,7 @@ int run_once(const pcg_hydro_params* p, std::vector<BoxIn>& boxes, int first, in
   int rc = ensure_eos(p->nspec);
   if (rc) return rc;
   Layout L;
-  build_layout(L, boxes, p->nspec, p->precision_mode == PCG_PREC_MIXED);
+  build_layout(L, boxes, p);
   void* ws = nullptr;
   if (L.ws_bytes) CUDA_TRY(ws_alloc(&ws, L.ws_bytes, s));
   rebase_workspace(L, boxes, static_cast<char*>(ws));
@@ -814,7 +822,7 @@ int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t
     bs[b].internal_q = true;
   }
   Layout L;
-  build_layout(L, bs, prm->nspec, prm->precision_mode == PCG_PREC_MIXED);
+  build_layout(L, bs, prm);
   Tables T;
   pack_tables(L, T);
   *bytes = int64_t((L.ws_bytes + kAlign - 1) / kAlign * kAlign + T.bytes);
@@ -969,7 +977,7 @@ int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* bo
   }
   aux_segments(bx, P->aux_segs, P->aux_blocks);
   if (fuse) fuse_boxes(P->boxes);
-  build_layout(P->L, P->boxes, prm->nspec, prm->precision_mode == PCG_PREC_MIXED);
+  build_layout(P->L, P->boxes, prm);
   cudaError_t e = cudaSuccess;
   if (P->L.ws_bytes) e = cudaMalloc(&P->ws, P->L.ws_bytes);
   if (e != cudaSuccess) {
@@ -1178,7 +1186,7 @@ extern "C" int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t 
   std::vector<BoxIn> boxes(1);
   if ((rc = box_from_desc(b, pcg::nvar(prm->nspec), boxes[0]))) return rc;
   Layout L;
-  build_layout(L, boxes, prm->nspec, prm->precision_mode == PCG_PREC_MIXED);
+  build_layout(L, boxes, prm);
   // scratch = [tables | workspace]; the table size does not depend on the addresses
   Tables T;
   pack_tables(L, T);

@@ -166,9 +166,10 @@ __global__ void __launch_bounds__(128, MINB) k_ctoprim(pcg::StageArgs a) {
   qa[pcg::QC] = cs;
   qa[pcg::QCSML] = dmax(pcg::SMALL_NUM, pcg::SMALL_NUM * cs);
   qa[pcg::QRSPEC] = pcg::RU / wbar;
-  // mixed form: the FP32 primitive copy the trace reads, on grow(box,3)
-  if (rg.qf.p && !rg.qf_in_prep && it.i >= rg.lo[0] - 3 && it.i <= rg.hi[0] + 3 && it.j >= rg.lo[1] - 3 &&
-      it.j <= rg.hi[1] + 3 && it.k >= rg.lo[2] - 3 && it.k <= rg.hi[2] + 3) {
+  // mixed form: the FP32 primitive copy the trace reads, on grow(box, qf_grow)
+  const int gq = rg.qf_grow;
+  if (rg.qf.p && !rg.qf_in_prep && it.i >= rg.lo[0] - gq && it.i <= rg.hi[0] + gq && it.j >= rg.lo[1] - gq &&
+      it.j <= rg.hi[1] + gq && it.k >= rg.lo[2] - gq && it.k <= rg.hi[2] + gq) {
     const double p0 = p0_of<NS, MIX, float>(rg);
     const CellPtr<float> f = at(v4<float>(rg.qf), it.i, it.j, it.k);
     f[pcg::TR_RHO] = float(rho);
@@ -274,10 +275,12 @@ template <> struct Prim<double> {
     st = dstride(v, d);
   }
   __device__ __forceinline__ double c(int qcomp) const { return p[qcomp * ns]; }
-  __device__ __forceinline__ void five(int qcomp, double* s) const {
+  __device__ __forceinline__ void five(int qcomp, double* s) const { stencil<2>(qcomp, s); }
+  template <int W>
+  __device__ __forceinline__ void stencil(int qcomp, double* s) const {
     const double* b = p + qcomp * ns;
 #pragma unroll
-    for (int o = -2; o <= 2; ++o) s[o + 2] = b[o * st];
+    for (int o = -W; o <= W; ++o) s[o + W] = b[o * st];
   }
 };
 template <> struct Prim<float> {
@@ -290,32 +293,65 @@ template <> struct Prim<float> {
     st = dstride(v, d);
   }
   __device__ __forceinline__ float c(int qcomp) const { return p[tr_comp(qcomp) * ns]; }
-  __device__ __forceinline__ void five(int qcomp, float* s) const {
+  __device__ __forceinline__ void five(int qcomp, float* s) const { stencil<2>(qcomp, s); }
+  template <int W>
+  __device__ __forceinline__ void stencil(int qcomp, float* s) const {
     const float* b = p + tr_comp(qcomp) * ns;
 #pragma unroll
-    for (int o = -2; o <= 2; ++o) s[o + 2] = b[o * st];
+    for (int o = -W; o <= W; ++o) s[o + W] = b[o * st];
   }
 };
+
+// Edge values sm, sp and centre value sc of component qcomp of the cell for the PPM
+// trace: the PPM parabola (Source/PPM.H:28-115), or with HYB the hybrid-WENO edge values
+// of Source/PPM.cpp:120-172 (weno_scheme 0 WENO-JS5, 1 WENO-Z5, 2 WENO-Z7, 3 WENO-Z3,
+// any other value the PPM parabola).
+template <bool HYB, class R>
+__device__ __forceinline__ void ppm_edges(const Prim<R>& P, int qcomp, R flat, int scheme, R& sm, R& sp, R& sc) {
+  if constexpr (HYB) {
+    if (scheme == 2) {
+      R s7[7];
+      P.template stencil<3>(qcomp, s7);
+      weno::weno7z<R>(s7, sm, sp);
+      sc = s7[3];
+      return;
+    }
+    if (scheme == 3) {
+      R s3[3];
+      P.template stencil<1>(qcomp, s3);
+      weno::weno3z<R>(s3, sm, sp);
+      sc = s3[1];
+      return;
+    }
+  }
+  R s[5];
+  P.five(qcomp, s);
+  if (HYB && (scheme == 0 || scheme == 1))
+    weno::weno5<R>(s, scheme == 1, sm, sp);
+  else
+    ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);
+  sc = s[2];
+}
 
 // Source/PPM.cpp:82-423 for one cell and direction D (bx == vbx as called from
 // Source/Godunov.cpp:188-200, so both states are produced). Only the components the
 // path reads are reconstructed: QGAME, QREINT and QTEMP profiles feed nothing.
-template <int NS, bool MIX, bool EXACT, int D, class R>
-__device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, double dt) {
+template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R>
+__device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, double dt,
+                                              int scheme) {
   using E = Eos<NS, MIX, R>;
   using ER = EosR<NS, MIX, R>;
   const Prim<R> P(rg, i, j, k, D);
   const R dtdx = R(dt / rg.dx[D]);
   const R un = P.c(pcg::QU + D);
-  R s[5], sm, sp, s6;
+  R sm, sp, sc, s6;
   R Imr[3], Ipr[3], Imu[3], Ipu[3], Imp[3], Ipp[3];
   R Imt[3], Ipt[3];
   const R sp3[3] = {un - cc, un, un + cc};
   const R p0 = R(p0_of<NS, MIX, R>(rg));
 #define PROFILE3(comp, Im, Ip)                                      \
-  P.five(comp, s);                                                   \
-  ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);    \
-  s6 = ppm_s6<R>(sm, sp, s[2]);                                      \
+  ppm_edges<HYB, R>(P, comp, flat, scheme, sm, sp, sc);              \
+  s6 = ppm_s6<R>(sm, sp, sc);                                        \
   _Pragma("unroll") for (int w = 0; w < 3; ++w) ppm_wave<R>(sm, sp, s6, sp3[w], dtdx, Ip[w], Im[w]);
   PROFILE3(pcg::QRHO, Imr, Ipr)
   PROFILE3(pcg::QU + D, Imu, Ipu)
@@ -323,9 +359,8 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (c == D) continue;
-    P.five(pcg::QU + c, s);
-    ppm_reconstruct<R>(s[0], s[1], s[2], s[3], s[4], flat, sm, sp);
-    s6 = ppm_s6<R>(sm, sp, s[2]);
+    ppm_edges<HYB, R>(P, pcg::QU + c, flat, scheme, sm, sp, sc);
+    s6 = ppm_s6<R>(sm, sp, sc);
     ppm_wave<R>(sm, sp, s6, un, dtdx, Ipt[c], Imt[c]);
   }
   R ym0[NS], ym1[NS], yp1[NS], yp2[NS];
@@ -514,13 +549,13 @@ __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int 
                           at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2)));
 }
 
-template <int NS, bool MIX, bool EXACT, int D, class R>
+template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R>
 __device__ __forceinline__ void trace_cell(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
   const CellPtr<const R> pr = at(v4<const R>(rg.prep), i, j, k);
   const R flat = pr[0], cc = pr[1];
   const double dt = dt_of(a, rg);
   if (a.ppm_type == 1)
-    trace_ppm_dir<NS, MIX, EXACT, D, R>(rg, i, j, k, cc, flat, dt);
+    trace_ppm_dir<NS, MIX, EXACT, HYB, D, R>(rg, i, j, k, cc, flat, dt, a.weno_scheme);
   else
     trace_plm_dir<NS, MIX, D, R>(rg, i, j, k, cc, flat, a.plm_iorder, dt);
 }
@@ -530,9 +565,22 @@ __global__ void __launch_bounds__(128, MINB) k_trace(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   switch (it.variant) {
-    case 0: trace_cell<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
-    case 1: trace_cell<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
-    default: trace_cell<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 0: trace_cell<NS, MIX, EXACT, false, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: trace_cell<NS, MIX, EXACT, false, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+    default: trace_cell<NS, MIX, EXACT, false, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  }
+}
+
+// The PPM trace with hybrid-WENO edge values (use_hybrid_weno): its own kernel, so that
+// the WENO code does not weigh on the registers of the plain trace.
+template <int NS, bool MIX, bool EXACT, class R>
+__global__ void __launch_bounds__(128) k_trace_weno(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  switch (it.variant) {
+    case 0: trace_cell<NS, MIX, EXACT, true, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: trace_cell<NS, MIX, EXACT, true, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
+    default: trace_cell<NS, MIX, EXACT, true, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
   }
 }
 

@@ -96,7 +96,7 @@ struct Region {
   int32_t zero_uout; // 1: write uout (=), 0: accumulate (+=)
   int32_t qf_in_prep; // 1: k_prep writes qf (no ctoprim stage), 0: k_ctoprim writes it
   int32_t ff_single;  // 1: ff/qec are FP32 with the pressure as deviation from p0
-  int32_t pad2;
+  int32_t qf_grow;    // qf covers grow(box, qf_grow): 3, or 4 for the 7-point WENO trace
 };
 
 // A run of thread blocks of one stage working on one region (and one variant, e.g.
@@ -131,6 +131,9 @@ struct StageArgs {
   int32_t ppm_type;
   int32_t plm_iorder;
   int32_t use_flattening;
+  int32_t use_hybrid_weno;
+  int32_t weno_scheme;
+  int32_t pad;
   double difmag;
   const double* dt_dev;  // nullptr: each region's dt
 };

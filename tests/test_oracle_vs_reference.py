@@ -63,3 +63,31 @@ def test_oracle_equals_reference_build_with_domain_boundaries(bc, nspec, ppm):
     np.testing.assert_array_equal(a.data, b.data)
     for d in range(3):
         np.testing.assert_array_equal(fa[d].data, fb[d].data)
+
+
+@pytest.mark.parametrize("scheme", [0, 1, 2, 3])
+@pytest.mark.parametrize("nspec", [1, 9])
+@pytest.mark.parametrize("seed", [401, 402])
+def test_oracle_equals_reference_build_hybrid_weno(scheme, nspec, seed):
+    """PPM with hybrid WENO edge values (Source/PPM.cpp:120-172, Source/WENO.H):
+    WENO-JS5 (0), WENO-Z5 (1), WENO-Z7 (2), WENO-Z3 (3)."""
+    if not pyoracle.ref_available(nspec):
+        pytest.skip("oracle/_ref not built (needs the reference checkout)")
+    eos = wl.GammaLaw() if nspec == 1 else eos9()
+    p = wl.random_patch((6, 5, 7), seed, eos if nspec == 9 else None)
+    ref = pyoracle.reference(nspec)
+    ref.set_eos(eos)
+    o = oracle()
+    o.set_eos(eos)
+    dt = 0.3 * ref.estdt(p.lo, p.hi, p.fab, p.dx)
+    prm = abi.make_params(p.dx, dt, nspec, (-BIG,) * 3, (BIG,) * 3, (0, 0, 0), (0, 0, 0), ppm_type=1)
+    prm.use_hybrid_weno = 1
+    prm.weno_scheme = scheme
+    a, fa = o.hydro_box(prm, p.lo, p.hi, p.fab)
+    b, fb = ref.hydro_box(prm, p.lo, p.hi, p.fab)
+    np.testing.assert_array_equal(a.data, b.data)
+    for d in range(3):
+        np.testing.assert_array_equal(fa[d].data, fb[d].data)
+    prm.use_hybrid_weno = 0
+    c, _ = o.hydro_box(prm, p.lo, p.hi, p.fab)
+    assert not np.array_equal(a.data, c.data)  # the WENO branch was taken

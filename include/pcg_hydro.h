@@ -207,6 +207,14 @@ int pcg_plan_stages(pcg_plan* plan, int32_t first, int32_t last, const double* d
 int pcg_plan_estdt(pcg_plan* plan, double cfl, double* dt_dev, pcg_stream_t stream);
 /* S_new = S_old + dt * hydro_source in place in each box's uin, then computeTemp. */
 int pcg_plan_update(pcg_plan* plan, const double* dt_dev, pcg_stream_t stream);
+/* One level step after the ghost fill with timestep *dt_dev (device): the hydro stages,
+ * then in one pass per cell the flux divergence, S_new = S_old + dt * hydro_source with
+ * computeTemp (in place in each box's uin) and the CFL minimum of S_new; *dt_next
+ * (device, may equal dt_dev) receives cfl * that minimum, the next step's timestep
+ * (PeleC's estTimeStep at the start of the next step, Source/PeleC.cpp:829-960, reads the
+ * same valid cells). The hydro source arrays (uout) are not written. Same results as
+ * pcg_plan_hydro + pcg_plan_update followed by pcg_plan_estdt. */
+int pcg_plan_advance(pcg_plan* plan, double cfl, const double* dt_dev, double* dt_next, pcg_stream_t stream);
 int pcg_plan_info(const pcg_plan* plan, int64_t* workspace_bytes, int32_t* nregions,
                   int64_t* blocks_per_stage /* [7] */);
 int pcg_plan_destroy(pcg_plan* plan);

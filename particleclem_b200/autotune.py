@@ -1,7 +1,8 @@
 """Launch-shape autotuner for the hydro stages.
 
-Every heavy stage (ctoprim, trace, the three Riemann stages) is compiled in three
-register budgets (``kMinBlocks`` in csrc/pcg_kernels.cuh: no cap, moderate, tight),
+Every heavy stage (ctoprim, trace, the three Riemann stages, and the fused step tail
+that the consup slot selects for ``pcg_plan_advance``) is compiled in three register
+budgets (``kMinBlocks`` in csrc/pcg_kernels.cuh: no cap, moderate, tight),
 which trades registers per thread against resident warps per SM. The best choice
 depends on the precision form (FP32 or FP64 arithmetic), the species count and the GPU,
 so it is measured: :func:`tune` runs each variant of each stage on a live plan with
@@ -17,6 +18,7 @@ from . import native
 
 TUNED_STAGES = (0, 2, 3, 4, 5)  # ctoprim, trace, flux0, flux1, flux2
 STAGE_NAMES = ("ctoprim", "prep", "trace", "flux0", "flux1", "flux2", "consup")
+TAIL_STAGE = 6  # the consup slot: its variant selects the fused step tail's register cap
 NVARIANT = 3
 
 
@@ -31,10 +33,12 @@ def set_variant(prec, nspec, stage, variant):
     native.call("pcg_set_launch_variant", int(prec), int(nspec), int(stage), int(variant))
 
 
-def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES):
+def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES, state=None):
     """Time every variant of ``stages`` on ``plan`` (a hydro.Plan whose workspace holds
     a valid state; stages before each tuned one are run once first) and install the
-    fastest. Returns {stage_name: {"variant": v, "ms": [ms per variant]}}."""
+    fastest. With ``state`` (the device tensor the plan's boxes update) the fused step
+    tail is tuned too: whole ``plan.advance`` calls per variant, the state restored
+    afterwards. Returns {stage_name: {"variant": v, "ms": [ms per variant]}}."""
     import torch
 
     prec, ns = plan.prm.precision_mode, plan.prm.nspec
@@ -42,17 +46,27 @@ def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES):
     torch.cuda.synchronize()
     result = {}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if state is not None:
+        stages = tuple(stages) + (TAIL_STAGE,)
+        saved = state.clone()
+        dt_next = torch.zeros(1, dtype=torch.float64, device=state.device)
     for st in stages:
         times = []
         for v in range(NVARIANT):
             set_variant(prec, ns, st, v)
-            plan.stages(st, st, dt_dev)  # warm
+            if st == TAIL_STAGE:
+                run = lambda: plan.advance(1.0, dt_dev, dt_next)  # noqa: E731
+            else:
+                run = lambda: plan.stages(st, st, dt_dev)  # noqa: E731
+            run()  # warm
             e0.record()
             for _ in range(reps):
-                plan.stages(st, st, dt_dev)
+                run()
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / reps)
+            if st == TAIL_STAGE:
+                state.copy_(saved)
         best = min(range(NVARIANT), key=lambda v: times[v])
         set_variant(prec, ns, st, best)
         result[STAGE_NAMES[st]] = {"variant": best, "ms": [round(t, 4) for t in times]}

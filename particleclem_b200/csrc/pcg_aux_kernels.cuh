@@ -3,7 +3,7 @@
 // ghost fill. All FP64.
 #pragma once
 
-#include "pcg_device.cuh"
+#include "pcg_kernels.cuh"
 
 namespace PCG_TU {
 
@@ -42,28 +42,40 @@ __device__ __forceinline__ double block_min(double v) {
   return v;
 }
 
-// Source/Timestep.H:51-88 (pc_estdt_hydro): per-cell dx_d / (c + |u_d|), block minima.
+// Source/Timestep.H:51-88 (pc_estdt_hydro) for one cell of state s:
+// min over d of dx_d / (c + |u_d|), c from the stored temperature.
+template <int NS, bool MIX>
+__device__ __forceinline__ double cfl_dt(const double* s, const double* dx) {
+  using E = Eos<NS, MIX, double>;
+  const double rho = s[pcg::URHO];
+  const double rhoInv = 1.0 / rho;
+  const double T = s[pcg::UTEMP];
+  double y[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) y[n] = s[pcg::UFS + n] * rhoInv;
+  const double c = E::rty2cs(rho, T, y);
+  double dt = DBL_MAX;
+  const double ux = s[pcg::UMX] * rhoInv;
+  dt = dmin(dt, dx[0] / (c + fabs(ux)));
+  const double uy = s[pcg::UMY] * rhoInv;
+  dt = dmin(dt, dx[1] / (c + fabs(uy)));
+  const double uz = s[pcg::UMZ] * rhoInv;
+  dt = dmin(dt, dx[2] / (c + fabs(uz)));
+  return dt;
+}
+
+// Per-cell CFL constraints of every valid cell, block minima.
 template <int NS, bool MIX>
 __global__ void __launch_bounds__(128) k_estdt(pcg::AuxArgs a) {
   const pcg::AuxBox* bx;
   int i, j, k;
   double dt = DBL_MAX;
   if (aux_item(a, bx, i, j, k)) {
-    using E = Eos<NS, MIX, double>;
     const V4<const double> u = v4<const double>(bx->uin);
-    const double rho = u(i, j, k, pcg::URHO);
-    const double rhoInv = 1.0 / rho;
-    const double T = u(i, j, k, pcg::UTEMP);
-    double y[NS];
+    double s[pcg::nvar(NS)];
 #pragma unroll
-    for (int n = 0; n < NS; ++n) y[n] = u(i, j, k, pcg::UFS + n) * rhoInv;
-    const double c = E::rty2cs(rho, T, y);
-    const double ux = u(i, j, k, pcg::UMX) * rhoInv;
-    dt = dmin(dt, bx->dx[0] / (c + fabs(ux)));
-    const double uy = u(i, j, k, pcg::UMY) * rhoInv;
-    dt = dmin(dt, bx->dx[1] / (c + fabs(uy)));
-    const double uz = u(i, j, k, pcg::UMZ) * rhoInv;
-    dt = dmin(dt, bx->dx[2] / (c + fabs(uz)));
+    for (int n = 0; n < pcg::nvar(NS); ++n) s[n] = u(i, j, k, n);
+    dt = cfl_dt<NS, MIX>(s, bx->dx);
   }
   dt = block_min(dt);
   if (threadIdx.x == 0) a.partial[blockIdx.x] = dt;
@@ -79,23 +91,12 @@ __global__ void __launch_bounds__(128) k_estdt_final(pcg::AuxArgs a) {
 
 // Source/Advance.cpp:397-417 (construct_Snew, hydro only) then Source/PeleC.cpp:2289-2305
 // (computeTemp): pc_rst_int_e default branch (PeleCUtilities.H:227-235) and pc_cmpTemp
-// (PeleCUtilities.H:70-84).
+// (PeleCUtilities.H:70-84), on one cell: s holds S_old on entry and S_new on exit.
 template <int NS, bool MIX>
-__global__ void __launch_bounds__(128) k_update(pcg::AuxArgs a) {
-  const pcg::AuxBox* bx;
-  int i, j, k;
-  if (!aux_item(a, bx, i, j, k)) return;
+__device__ __forceinline__ void update_cell(double* s, const double* hsrc, double dt) {
   using E = Eos<NS, MIX, double>;
-  const double dt = a.dt_in ? *a.dt_in : bx->dt;
-  const V4<const double> so = v4<const double>(bx->uin);
-  const V4<const double> hs = v4<const double>(bx->uout);
-  const V4<double> sn = v4<double>(bx->snew);
-  double s[pcg::nvar(NS)];
 #pragma unroll
-  for (int n = 0; n < pcg::nvar(NS); ++n) {
-    s[n] = so(i, j, k, n);
-    s[n] += dt * hs(i, j, k, n);
-  }
+  for (int n = 0; n < pcg::nvar(NS); ++n) s[n] += dt * hsrc[n];
   const double rho = s[pcg::URHO];
   const double rhoInv = 1.0 / rho;
   const double Up = s[pcg::UMX] * rhoInv;
@@ -109,8 +110,55 @@ __global__ void __launch_bounds__(128) k_update(pcg::AuxArgs a) {
 #pragma unroll
   for (int n = 0; n < NS; ++n) y[n] = s[pcg::UFS + n] * rhoInv2;
   s[pcg::UTEMP] = E::rey2t(e, y, s[pcg::UTEMP]);
+}
+
+template <int NS, bool MIX>
+__global__ void __launch_bounds__(128) k_update(pcg::AuxArgs a) {
+  const pcg::AuxBox* bx;
+  int i, j, k;
+  if (!aux_item(a, bx, i, j, k)) return;
+  const double dt = a.dt_in ? *a.dt_in : bx->dt;
+  const V4<const double> so = v4<const double>(bx->uin);
+  const V4<const double> hs = v4<const double>(bx->uout);
+  const V4<double> sn = v4<double>(bx->snew);
+  double s[pcg::nvar(NS)], h[pcg::nvar(NS)];
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) {
+    s[n] = so(i, j, k, n);
+    h[n] = hs(i, j, k, n);
+  }
+  update_cell<NS, MIX>(s, h, dt);
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) sn(i, j, k, n) = s[n];
+}
+
+// The tail of a level step in one pass over the cells of each region: the flux
+// divergence and p div u of pc_consup (kept in registers, the hydro source array is not
+// written), S_new = S_old + dt * hydro_source with computeTemp written over the state in
+// place, and the CFL constraint of S_new for the next step (block minima; the final
+// minimum is k_estdt_final). Each value is formed by the same expressions as k_consup,
+// k_update and k_estdt, so the step is the unfused step's.
+template <int NS, bool MIX, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_advance(pcg::StageArgs a) {
+  Item it;
+  double dtc = DBL_MAX;
+  if (item_of(a, it)) {
+    const pcg::Region& rg = *it.rg;
+    double h[pcg::nvar(NS)], s[pcg::nvar(NS)];
+    if (rg.ff_single)
+      consup_sum<NS, float>(rg, it.i, it.j, it.k, p0_of<NS, MIX, float>(rg), h);
+    else
+      consup_sum<NS, double>(rg, it.i, it.j, it.k, 0.0, h);
+    const CellPtr<double> u = at(v4<double>(rg.uin), it.i, it.j, it.k);
+#pragma unroll
+    for (int n = 0; n < pcg::nvar(NS); ++n) s[n] = u[n];
+    update_cell<NS, MIX>(s, h, dt_of(a, rg));
+#pragma unroll
+    for (int n = 0; n < pcg::nvar(NS); ++n) u[n] = s[n];
+    dtc = cfl_dt<NS, MIX>(s, rg.dx);
+  }
+  dtc = block_min(dtc);
+  if (threadIdx.x == 0) a.partial[blockIdx.x] = dtc;
 }
 
 // Single-level FillBoundary of one direction: the ghost slabs of a domain FAB that
@@ -141,6 +189,19 @@ __global__ void __launch_bounds__(128) k_fill(pcg::AuxArgs a) {
   }
   const V4<double> s = v4<double>(a.state);
   for (int comp = 0; comp < a.ncomp; ++comp) s(dst[0], dst[1], dst[2], comp) = s(src[0], src[1], src[2], comp);
+}
+
+template <int NS, bool MIX>
+static cudaError_t launch_advance_t(const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
+  if (nblocks <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)nblocks), block(128);
+  switch (variant) {
+    case 0: k_advance<NS, MIX, kMinBlocks[K_CONSUP][0]><<<grid, block, 0, s>>>(a); break;
+    case 1: k_advance<NS, MIX, kMinBlocks[K_CONSUP][1]><<<grid, block, 0, s>>>(a); break;
+    case 2: k_advance<NS, MIX, kMinBlocks[K_CONSUP][2]><<<grid, block, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 template <int NS, bool MIX>

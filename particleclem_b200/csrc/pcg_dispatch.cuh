@@ -72,6 +72,12 @@ cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
+  if (ns == 1) return launch_advance_t<1, false>(a, nblocks, variant, s);
+  if (ns == 9) return launch_advance_t<9, true>(a, nblocks, variant, s);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s) {
   if (ns == 1) return launch_aux_t<1, false>(which, a, nblocks, s);
   if (ns == 9) return launch_aux_t<9, true>(which, a, nblocks, s);

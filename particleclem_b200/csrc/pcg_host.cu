@@ -24,12 +24,14 @@
 
 namespace pcg_strict {
 cudaError_t upload_eos(int slot, const pcg::EosConst& e);
+cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s);
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
                          cudaStream_t s);
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
 }  // namespace pcg_strict
 namespace pcg_fast {
 cudaError_t upload_eos(int slot, const pcg::EosConst& e);
+cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s);
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
                          cudaStream_t s);
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
@@ -52,9 +54,9 @@ thread_local std::string g_err;
 // level; pcg_set_launch_variant (the autotuner) overrides them.
 std::mutex g_var_mu;
 int g_variant[3][2][7] = {
-  {{0, 0, 2, 0, 2, 2, 0}, {2, 0, 1, 1, 2, 0, 0}},  // FP64 reference order
-  {{2, 0, 1, 0, 0, 0, 0}, {2, 0, 1, 0, 0, 0, 0}},  // FP64 with FMA
-  {{0, 0, 2, 0, 2, 0, 0}, {2, 0, 2, 2, 2, 1, 0}},  // mixed
+  {{0, 0, 2, 0, 2, 2, 2}, {2, 0, 1, 1, 2, 0, 2}},  // FP64 reference order
+  {{2, 0, 1, 0, 0, 0, 2}, {2, 0, 1, 0, 0, 0, 2}},  // FP64 with FMA
+  {{0, 0, 2, 0, 2, 0, 2}, {2, 0, 2, 2, 2, 1, 2}},  // mixed
 };
 int variant_of(int prec, int ns, int stage) {
   std::lock_guard<std::mutex> lk(g_var_mu);
@@ -988,7 +990,7 @@ int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* bo
   rebase_workspace(P->L, P->boxes, static_cast<char*>(P->ws));
   pack_tables(P->L, P->T);
   const size_t b1 = P->aux.size() * sizeof(pcg::AuxBox), b2 = P->aux_segs.size() * sizeof(pcg::Seg),
-               b3 = P->aux_blocks * sizeof(double);
+               b3 = std::max<int64_t>(P->aux_blocks, P->L.nblocks[K_CONSUP]) * sizeof(double);
   if ((e = cudaMalloc(&P->T.dev, P->T.bytes)) == cudaSuccess &&
       (e = cudaMemcpy(P->T.dev, P->T.host.data(), P->T.bytes, cudaMemcpyHostToDevice)) == cudaSuccess &&
       (e = cudaMalloc(&P->aux_dev, b1 + b2 + b3)) == cudaSuccess) {
@@ -1060,13 +1062,41 @@ int pcg_plan_update(pcg_plan* P, const double* dt_dev, pcg_stream_t stream) {
   return e == cudaSuccess ? PCG_OK : fail(PCG_ECUDA, "update: %s", cudaGetErrorString(e));
 }
 
+int pcg_plan_advance(pcg_plan* P, double cfl, const double* dt_dev, double* dt_next, pcg_stream_t stream) {
+  if (!P || !dt_dev || !dt_next) return fail(PCG_EINVAL, "bad arguments");
+  int rc = ensure_eos(P->prm.nspec);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if ((rc = launch_stages(P->L, P->T, &P->prm, K_CTOPRIM, K_FLUX2, dt_dev, s))) return rc;
+  pcg::StageArgs a{};
+  a.regions = P->T.regions;
+  a.segs = P->T.segs[K_CONSUP];
+  a.nseg = (int32_t)P->L.segs[K_CONSUP].size();
+  a.dt_dev = dt_dev;
+  a.partial = P->d_partial;
+  const int64_t nb = P->L.nblocks[K_CONSUP];
+  const int v = variant_of(P->prm.precision_mode, P->prm.nspec, K_CONSUP);
+  cudaError_t e = (P->prm.precision_mode == PCG_PREC_FP64) ? pcg_strict::launch_advance(P->prm.nspec, a, nb, v, s)
+                                                           : pcg_fast::launch_advance(P->prm.nspec, a, nb, v, s);
+  if (e == cudaSuccess) {
+    pcg::AuxArgs f{};
+    f.partial = P->d_partial;
+    f.npartial = nb;
+    f.cfl = cfl;
+    f.dt_out = dt_next;
+    e = pcg_strict::launch_aux(AUX_ESTDT_FINAL, P->prm.nspec, f, 1, s);
+  }
+  return e == cudaSuccess ? PCG_OK : fail(PCG_ECUDA, "advance: %s", cudaGetErrorString(e));
+}
+
 int pcg_plan_info(const pcg_plan* P, int64_t* workspace_bytes, int32_t* nregions, int64_t* blocks_per_stage) {
   if (!P) return fail(PCG_EINVAL, "plan is NULL");
   if (workspace_bytes) *workspace_bytes = (int64_t)P->L.ws_bytes;
   if (nregions) *nregions = (int32_t)P->L.regions.size();
-  if (blocks_per_stage)
+  if (blocks_per_stage) {
     for (int s = 0; s < K_NSTAGE; ++s) blocks_per_stage[s] = P->L.nblocks[s];
     blocks_per_stage[K_FLUX2] += P->L.nblocks[K_LOWBC];
+  }
   return PCG_OK;
 }
 

@@ -38,7 +38,7 @@ constexpr int kMinBlocks[K_NSTAGE][3] = {
   {0, 6, 8},  // flux0
   {4, 5, 6},  // flux1
   {4, 5, 6},  // flux2
-  {0, 0, 0},  // consup
+  {0, 4, 5},  // consup: the caps apply to the fused step tail (k_advance)
 };
 
 struct Item {
@@ -1253,7 +1253,7 @@ __global__ void __launch_bounds__(128) k_lowbc(pcg::StageArgs a) {
 // pressure as deviation from p0; p0 cancels in the flux differences and is added back to
 // the Godunov pressures of pdivu).
 template <int NS, class F>
-__device__ __forceinline__ void consup_cell(const pcg::Region& rg, int i, int j, int k, double p0) {
+__device__ __forceinline__ void consup_sum(const pcg::Region& rg, int i, int j, int k, double p0, double* h) {
   const V4<const F> f0v = v4<const F>(rg.ff[0]), f1v = v4<const F>(rg.ff[1]), f2v = v4<const F>(rg.ff[2]);
   const CellPtr<const F> f0 = at(f0v, i, j, k), f1 = at(f1v, i, j, k), f2 = at(f2v, i, j, k);
   const CellPtr<const F> f0p = shift(f0, 1), f1p = shift(f1, f1v.js), f2p = shift(f2, f2v.ks);
@@ -1277,11 +1277,20 @@ __device__ __forceinline__ void consup_cell(const pcg::Region& rg, int i, int j,
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) {
     const double old = rg.zero_uout ? 0.0 : uo[n];
-    uo[n] = old + (double(f0[n]) - double(f0p[n]) + double(f1[n]) - double(f1p[n]) + double(f2[n]) -
-                   double(f2p[n])) /
-                      v;
+    h[n] = old + (double(f0[n]) - double(f0p[n]) + double(f1[n]) - double(f1p[n]) + double(f2[n]) -
+                  double(f2p[n])) /
+                     v;
   }
-  uo[pcg::UEINT] -= pdivu;
+  h[pcg::UEINT] -= pdivu;
+}
+
+template <int NS, class F>
+__device__ __forceinline__ void consup_cell(const pcg::Region& rg, int i, int j, int k, double p0) {
+  double h[pcg::nvar(NS)];
+  consup_sum<NS, F>(rg, i, j, k, p0, h);
+  const CellPtr<double> uo = at(v4<double>(rg.uout), i, j, k);
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) uo[n] = h[n];
 }
 
 template <int NS, bool MIX>

@@ -136,6 +136,7 @@ struct StageArgs {
   int32_t pad;
   double difmag;
   const double* dt_dev;  // nullptr: each region's dt
+  double* partial;       // fused step tail: one timestep minimum per block
 };
 
 // One box for the auxiliary kernels (timestep, state update).

@@ -151,6 +151,12 @@ class Plan:
     def estdt(self, cfl, dt_dev, stream=None):
         native.call("pcg_plan_estdt", self.h, float(cfl), C.c_void_p(dt_dev.data_ptr()), _stream_ptr(stream))
 
+    def advance(self, cfl, dt_dev, dt_next, stream=None):
+        """Hydro stages and the fused update with this step's dt_dev; dt_next receives
+        the next step's CFL timestep (both one-element CUDA float64 tensors)."""
+        native.call("pcg_plan_advance", self.h, float(cfl), C.c_void_p(dt_dev.data_ptr()),
+                    C.c_void_p(dt_next.data_ptr()), _stream_ptr(stream))
+
     def update(self, dt_dev=None, stream=None):
         native.call("pcg_plan_update", self.h, C.c_void_p(dt_dev.data_ptr()) if dt_dev is not None else None,
                     _stream_ptr(stream))

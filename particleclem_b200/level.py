@@ -17,9 +17,17 @@ from . import abi, hydro
 NG = abi.NGROW
 
 
+class _nullctx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
 class LevelStepper:
     def __init__(self, level, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, ppm_type=1, plm_iorder=4,
-                 use_flattening=True, difmag=0.1, device=0):
+                 use_flattening=True, difmag=0.1, device=0, fused_tail=True):
         import torch
 
         self.torch = torch
@@ -35,6 +43,10 @@ class LevelStepper:
         self.hsrc = abi.Fab(torch.zeros((self.nv, n[2], n[1], n[0]), dtype=torch.float64, device=self.dev),
                             tuple(level.domlo))
         self.dt = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        # with the fused tail the step also produces the next step's timestep
+        self.fused_tail = bool(fused_tail)
+        self.dt_next = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self._primed = False
         self.prm = abi.make_params(level.dx, 0.0, self.ns, level.domlo, level.domhi, level.bclo, level.bchi,
                                    ppm_type=ppm_type, plm_iorder=plm_iorder, use_flattening=use_flattening,
                                    difmag=difmag, precision_mode=precision)
@@ -49,25 +61,49 @@ class LevelStepper:
         L = self.level
         hydro.fill_ghosts(self.state, L.domlo, L.domhi, L.periodic, NG, stream)
 
-    def step(self, stream=None):
+    def load_state(self, src, non_blocking=False):
+        """Replace the level state (ghost cells included) with ``src``. The next step then
+        takes its timestep from a fresh CFL reduction of the new state."""
+        self.state.data.copy_(src, non_blocking=non_blocking)
+        self._primed = False
+
+    def step(self, stream=None, fresh_dt=False):
+        """One level step; self.dt holds the step's timestep afterwards. With the fused
+        tail the CFL minimum of the new state is formed by the update pass itself; the
+        timestep comes from a separate reduction on the first step, after
+        :meth:`load_state`, and on every step when ``fresh_dt`` is set (a step whose
+        state is written from outside between steps, as in a captured graph that is
+        replayed on new inputs)."""
         self.fill(stream)
-        self.plan.estdt(self.cfl, self.dt, stream)
-        self.plan.hydro(self.dt, stream)
-        self.plan.update(self.dt, stream)
+        if not self.fused_tail:
+            self.plan.estdt(self.cfl, self.dt, stream)
+            self.plan.hydro(self.dt, stream)
+            self.plan.update(self.dt, stream)
+            return
+        if fresh_dt or not self._primed:
+            self.plan.estdt(self.cfl, self.dt_next, stream)
+            self._primed = True
+        torch = self.torch
+        with torch.cuda.stream(stream) if stream is not None else _nullctx():
+            self.dt.copy_(self.dt_next)
+        self.plan.advance(self.cfl, self.dt, self.dt_next, stream)
 
-    launches_per_step = 3 + 2 + 7 + 1  # fill (3 directions), estdt (2), hydro stages, update
+    # fill (3 directions), hydro stages (6), fused consup/update/CFL minimum, final minimum
+    launches_per_step = 3 + 6 + 1 + 1
 
-    def capture(self):
+    def capture(self, fresh_dt=False):
+        """Capture one step as a CUDA graph (after one eager step that warms the library:
+        EOS upload, lazy module loading). ``fresh_dt`` as in :meth:`step`."""
         torch = self.torch
         s = torch.cuda.Stream(device=self.dev)
         s.wait_stream(torch.cuda.current_stream(self.dev))
         with torch.cuda.stream(s):
-            self.step()  # warm the library (EOS upload, lazy module loading) outside capture
+            self.step(fresh_dt=fresh_dt)
         torch.cuda.current_stream(self.dev).wait_stream(s)
         torch.cuda.synchronize(self.dev)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=s):
-            self.step()
+            self.step(fresh_dt=fresh_dt)
         self.graph = g
         return g
 
@@ -100,7 +136,7 @@ class HostPipeline:
         self.torch = torch
         self.slots = [LevelStepper(level, **stepper_kw) for _ in range(depth)]
         for s in self.slots:
-            s.capture()
+            s.capture(fresh_dt=True)  # every submission is a new state
         dev = self.slots[0].dev
         self.up, self.comp, self.down = (torch.cuda.Stream(device=dev) for _ in range(3))
         ev = lambda: [torch.cuda.Event() for _ in range(depth)]  # noqa: E731

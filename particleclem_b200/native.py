@@ -68,6 +68,7 @@ SIGNATURES = {
     "pcg_plan_stages": ([_V, C.c_int32, C.c_int32, _V, _V], C.c_int),
     "pcg_plan_estdt": ([_V, C.c_double, _V, _V], C.c_int),
     "pcg_plan_update": ([_V, _V, _V], C.c_int),
+    "pcg_plan_advance": ([_V, C.c_double, _V, _V, _V], C.c_int),
     "pcg_plan_info": ([_V, _P(C.c_int64), _P(C.c_int32), _P(C.c_int64)], C.c_int),
     "pcg_plan_destroy": ([_V], C.c_int),
     "pcg_set_launch_variant": ([C.c_int32, C.c_int32, C.c_int32, C.c_int32], C.c_int),

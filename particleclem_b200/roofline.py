@@ -121,7 +121,8 @@ def dominant_kernel_roofline(region_edges, ns, r, stage_names, stage_ms, pk, for
     tr = traffic_table(root).get(("k_" + st, form))
     return {"bound": "hbm", "kernel": "k_" + st, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": tr, "algorithmic_bytes_per_launch": byts,
-            "launch_ms": ms, "share_of_step": ms / sum(stage_ms), "peak_source": pk["source"]}
+            "launch_ms": ms, "share_of_step": ms / sum(v for n, v in zip(stage_names, stage_ms) if n != "advance"),
+            "peak_source": pk["source"]}
 
 
 def path_roofline(box_edges_list, ns, ms_per_step, pk):

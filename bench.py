@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline work budget")
     ap.add_argument("--serve-per-run", type=int, default=4, help="requests per ensemble run in the serving check")
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="only time the CPU baseline on the Sod box, the flame level and the turbulence level "
+                         "(PPM and PLM), one JSON line each")
     return ap.parse_args()
 
 
@@ -109,7 +112,7 @@ class CpuArm:
     box-parallel on all host threads (the reference tiles boxes over OpenMP threads,
     Source/Hydro.cpp:60-71). Each measurement is a bounded sample of one step's boxes."""
 
-    def __init__(self, level):
+    def __init__(self, level, ppm_type=1):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import pyoracle
         from particleclem_b200 import abi
@@ -120,7 +123,8 @@ class CpuArm:
         self.cores = len(os.sched_getaffinity(0))
         self.fabs = [(lo, hi, level.box_fab(lo, hi)) for lo, hi in level.boxes]
         dt = 0.3 * min(self.lib.estdt(lo, hi, f, level.dx) for lo, hi, f in self.fabs)
-        self.prm = abi.make_params(level.dx, dt, level.nspec, level.domlo, level.domhi, level.bclo, level.bchi)
+        self.prm = abi.make_params(level.dx, dt, level.nspec, level.domlo, level.domhi, level.bclo, level.bchi,
+                                   ppm_type=ppm_type)
         t0 = time.perf_counter()
         self.lib.hydro_box(self.prm, *self.fabs[0])
         self.t_box = time.perf_counter() - t0
@@ -129,16 +133,16 @@ class CpuArm:
     def measure(self, seconds):
         per_round = max(1, min(len(self.fabs), self.cores))
         rounds = max(1, int(seconds / max(self.t_box * 1.2, 1e-3)))
-        nbox = min(len(self.fabs), rounds * per_round)
-        work = self.fabs[:nbox]
+        nbox = rounds * per_round  # the step's boxes, repeated where the step is shorter than the budget
+        work = [self.fabs[b % len(self.fabs)] for b in range(nbox)]
         t0 = time.perf_counter()
         list(self.pool.map(lambda w: self.lib.hydro_box(self.prm, *w), work))
         el = time.perf_counter() - t0
         ncell = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h, _ in work)
         thr = min(self.cores, nbox)
         return {"value": ncell / el, "unit": UNIT, "cores": thr, "kind": self.kind,
-                "sample": f"{nbox} of the {len(self.fabs)} boxes of one step (construct_hydro_source incl. "
-                          f"ctoprim, FP64), {el:.1f} s on {thr} threads"}
+                "sample": f"{nbox} box advances over the {len(self.fabs)} boxes of one step "
+                          f"(construct_hydro_source incl. ctoprim, FP64), {el:.1f} s on {thr} threads"}
 
 
 def run_reference(args):
@@ -167,6 +171,36 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- our arm
+def run_cpu_configs(args):
+    """The CPU baseline on every level workload: the 32^3 Sod box (one species), the
+    128^3 flame level, the 256^3 turbulence level with PPM and with PLM."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from particleclem_b200 import workloads as wl
+
+    def sod_tiled():
+        # one 32^3 box, cut into the 32x8x8 tiles the reference's OpenMP box loop uses
+        # (AMReX default CPU tile size 1024x8x8), so that the box spreads over 16 threads
+        lev = wl.sod(n=32)
+        lev.boxes = wl.tile_boxes((32, 32, 32), (32, 8, 8))
+        return lev
+
+    cases = [("sod_32^3_ns1_ppm (32x8x8 tiles)", sod_tiled, 1),
+             (WORKLOAD, lambda: wl.flame(n=128, box=32, seed=2), 1),
+             ("turbulence_256^3_as_64x64^3_ns1_ppm", lambda: wl.turbulence(n=256, box=64, seed=4), 1),
+             ("turbulence_256^3_as_64x64^3_ns1_plm", lambda: wl.turbulence(n=256, box=64, seed=4), 0)]
+    for name, make, ppm in cases:
+        arm = CpuArm(make(), ppm_type=ppm)
+        arm.measure(min(2.0, args.cpu_seconds))  # warm
+        vals = [arm.measure(args.cpu_seconds / 3) for _ in range(3)]
+        vals.sort(key=lambda r: r["value"])
+        med = vals[1]
+        print(json.dumps({"config": {"workload": name}, "cpu_baseline": med,
+                          "runs": [round(r["value"]) for r in vals]}), flush=True)
+        arm.pool.shutdown()
+    return 0
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -335,32 +369,32 @@ def run_ours(args):
     if world == 1:
         host_in = torch.from_numpy(lev_e.state).pin_memory()
         host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
-        h2d = host_in.numel() * 8
-        d2h = host_out[0].numel() * 8
         se = LevelStepper(lev_e, precision=abi.PREC_MIXED, fuse=True)
+        h2d = d2h = se.row_bytes  # the valid rows each way; the step's ghost fill forms the rest
         for _ in range(2):
-            se.load_state(host_in, non_blocking=True)
+            se.upload(host_in)
             se.step()
-            host_out[0].copy_(se.state.data, non_blocking=True)
+            se.download(host_out[0])
         barrier()
         ke = max(1, min(args.steps, 5))
         e0.record()
         for _ in range(ke):
-            se.load_state(host_in, non_blocking=True)
+            se.upload(host_in)
             se.step()
-            host_out[0].copy_(se.state.data, non_blocking=True)
+            se.download(host_out[0])
         e1.record()
         barrier()
         mse_serial = max_over_ranks(e0.elapsed_time(e1))
         e2e_serial = world * ncell * ke / (mse_serial / 1e3)
         se.close()
 
-        pipe = HostPipeline(lev_e, depth=2, precision=abi.PREC_MIXED, fuse=True)
+        pipe = HostPipeline(lev_e, depth=3, precision=abi.PREC_MIXED, fuse=True)
+        assert (pipe.h2d_bytes, pipe.d2h_bytes) == (h2d, d2h)
         for i in range(3):
             pipe.submit(host_in, host_out[i % 2])
         pipe.synchronize()
         barrier()
-        kp = max(2, args.steps)
+        kp = max(20, args.steps)  # enough submissions that filling and draining the pipeline is amortised
         e0.record(pipe.up)
         for i in range(kp):
             pipe.submit(host_in, host_out[i % 2])
@@ -414,8 +448,9 @@ def run_ours(args):
             "error_vs_fp64": err,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": mse / kp, "steps": kp,
-                    "path": ("pinned host state -> H2D -> fill/estdt/hydro/update via C ABI -> D2H, every step; "
-                             "level.HostPipeline overlaps step k's compute with the copies of k+1 and k-1")
+                    "path": ("valid rows of a pinned host state -> H2D -> fill/estdt/hydro/update via C ABI -> "
+                             "valid rows D2H, every step; level.HostPipeline (3 device slots) overlaps the step of "
+                             "one submission with the upload of the next and the download of the previous")
                             if world == 1 else
                             "per rank: pinned host slab -> H2D -> slab step with halo exchange and dt all-reduce "
                             "-> D2H, every step",
@@ -444,6 +479,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.cpu_configs:
+        return run_cpu_configs(args)
     return run_ours(args)
 
 

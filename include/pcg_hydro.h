@@ -184,6 +184,16 @@ int pcg_update_state(int32_t nspec, int32_t nbox, const pcg_box* boxes,
 int pcg_fill_ghosts(const pcg_array4* state, const int32_t domlo[3], const int32_t domhi[3],
                     const int32_t periodic[3], int32_t ng, pcg_stream_t stream);
 
+/* Copy the cells [lo, hi] of every component from src to dst, two arrays of equal
+ * component count whose rows are contiguous (kstride a multiple of jstride); either may
+ * be host or device memory (unified addressing tells which; pinned host memory for an
+ * asynchronous copy). One strided copy per component, enqueued on stream. This moves a
+ * level's valid cells between a host FAB and the device FAB whose ghost cells
+ * pcg_fill_ghosts forms, so ghost cells do not cross the bus. No counterpart in the
+ * reference (AMReX moves a MultiFab's valid region with its own copy routines). */
+int pcg_copy_cells(const pcg_array4* src, const pcg_array4* dst, const int32_t lo[3], const int32_t hi[3],
+                   pcg_stream_t stream);
+
 /* ---- persistent plans (repeated steps, CUDA-graph capture) -------------------- */
 
 /* A plan fixes a box list and owns its workspace and launch tables, so that its run

@@ -946,6 +946,52 @@ int pcg_fill_ghosts(const pcg_array4* state, const int32_t domlo[3], const int32
   return PCG_OK;
 }
 
+int pcg_copy_cells(const pcg_array4* src, const pcg_array4* dst, const int32_t lo[3], const int32_t hi[3],
+                   pcg_stream_t stream) {
+  if (!src || !dst || !src->p || !dst->p || !lo || !hi) return fail(PCG_EINVAL, "bad arguments");
+  const IBox b = mkbox(lo, hi);
+  if (!b.ok()) return fail(PCG_EINVAL, "empty box");
+  if (src->ncomp != dst->ncomp) return fail(PCG_EINVAL, "component counts differ (%d, %d)", src->ncomp, dst->ncomp);
+  int rc = check_array("src", src, b, src->ncomp);
+  if (!rc) rc = check_array("dst", dst, b, dst->ncomp);
+  if (rc) return rc;
+  for (const pcg_array4* a : {src, dst})
+    if (a->jstride < a->end[0] - a->begin[0] || a->kstride % a->jstride || a->kstride / a->jstride < a->end[1] - a->begin[1])
+      return fail(PCG_EINVAL, "array rows must be contiguous with kstride a multiple of jstride");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // Whole rows in both arrays: each k-slice of the box is one contiguous run, so copy
+  // slices rather than rows (host-to-device copies of short strided rows run at a
+  // fraction of the bus bandwidth).
+  const bool whole_rows = b.n(0) == src->jstride && b.n(0) == dst->jstride;
+  for (int n = 0; n < src->ncomp && whole_rows; ++n) {
+    const double* sp = src->p + n * src->nstride + (lo[1] - src->begin[1]) * src->jstride +
+                       (int64_t)(lo[2] - src->begin[2]) * src->kstride;
+    double* dp = dst->p + n * dst->nstride + (lo[1] - dst->begin[1]) * dst->jstride +
+                 (int64_t)(lo[2] - dst->begin[2]) * dst->kstride;
+    cudaError_t e = cudaMemcpy2DAsync(dp, (size_t)dst->kstride * sizeof(double), sp,
+                                      (size_t)src->kstride * sizeof(double),
+                                      (size_t)(b.n(1) * b.n(0)) * sizeof(double), (size_t)b.n(2), cudaMemcpyDefault, s);
+    if (e != cudaSuccess) return fail(PCG_ECUDA, "copy_cells: %s", cudaGetErrorString(e));
+  }
+  if (whole_rows) return PCG_OK;
+  for (int n = 0; n < src->ncomp; ++n) {
+    cudaMemcpy3DParms c{};
+    c.srcPtr = make_cudaPitchedPtr(src->p + n * src->nstride, (size_t)src->jstride * sizeof(double),
+                                   (size_t)(src->end[0] - src->begin[0]), (size_t)(src->kstride / src->jstride));
+    c.dstPtr = make_cudaPitchedPtr(dst->p + n * dst->nstride, (size_t)dst->jstride * sizeof(double),
+                                   (size_t)(dst->end[0] - dst->begin[0]), (size_t)(dst->kstride / dst->jstride));
+    c.srcPos = make_cudaPos((size_t)(lo[0] - src->begin[0]) * sizeof(double), (size_t)(lo[1] - src->begin[1]),
+                            (size_t)(lo[2] - src->begin[2]));
+    c.dstPos = make_cudaPos((size_t)(lo[0] - dst->begin[0]) * sizeof(double), (size_t)(lo[1] - dst->begin[1]),
+                            (size_t)(lo[2] - dst->begin[2]));
+    c.extent = make_cudaExtent((size_t)b.n(0) * sizeof(double), (size_t)b.n(1), (size_t)b.n(2));
+    c.kind = cudaMemcpyDefault;
+    cudaError_t e = cudaMemcpy3DAsync(&c, s);
+    if (e != cudaSuccess) return fail(PCG_ECUDA, "copy_cells: %s", cudaGetErrorString(e));
+  }
+  return PCG_OK;
+}
+
 // ---- persistent plans ---------------------------------------------------------
 
 int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes, int32_t fuse, pcg_plan** out) {

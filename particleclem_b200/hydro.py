@@ -128,6 +128,12 @@ def fill_ghosts(state, domlo, domhi, periodic, ng=abi.NGROW, stream=None):
                 abi.ivec([int(bool(p)) for p in periodic]), int(ng), _stream_ptr(stream))
 
 
+def copy_cells(src, dst, lo, hi, stream=None):
+    """Copy the cells [lo, hi] of every component of FAB ``src`` into FAB ``dst`` (host
+    or device tensors; pinned host memory for an asynchronous copy), on ``stream``."""
+    native.call("pcg_copy_cells", _a4p(src), _a4p(dst), abi.ivec(lo), abi.ivec(hi), _stream_ptr(stream))
+
+
 class Plan:
     """Persistent launch plan over a fixed box list (graph-capturable runs)."""
 

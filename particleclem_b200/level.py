@@ -67,6 +67,32 @@ class LevelStepper:
         self.state.data.copy_(src, non_blocking=non_blocking)
         self._primed = False
 
+    def _valid_rows(self):
+        # the valid (j, k) rows, whole: x ghost cells included, so that the rows of one
+        # k-slice are one contiguous run (copies of short strided rows, host to device
+        # above all, run far below the bus bandwidth)
+        lo, hi = self.level.domlo, self.level.domhi
+        return (lo[0] - NG, lo[1], lo[2]), (hi[0] + NG, hi[1], hi[2])
+
+    def upload(self, host, stream=None):
+        """Copy the valid rows of ``host`` (a pinned tensor of the state's shape) into the
+        state; the step's ghost fill forms the ghost cells. The next step takes a fresh
+        CFL timestep."""
+        hydro.copy_cells(abi.Fab(host, self.state.lo), self.state, *self._valid_rows(), stream)
+        self._primed = False
+
+    def download(self, host, stream=None):
+        """Copy the valid rows of the state into ``host`` (pinned, the state's shape): the
+        valid cells, with the x ghost cells of those rows as the step's ghost fill left
+        them; the other ghost cells of ``host`` are not written."""
+        hydro.copy_cells(self.state, abi.Fab(host, self.state.lo), *self._valid_rows(), stream)
+
+    @property
+    def row_bytes(self):
+        """Bytes :meth:`upload` and :meth:`download` move."""
+        n = [self.level.domhi[d] - self.level.domlo[d] + 1 for d in range(3)]
+        return self.nv * (n[0] + 2 * NG) * n[1] * n[2] * 8
+
     def step(self, stream=None, fresh_dt=False):
         """One level step; self.dt holds the step's timestep afterwards. With the fused
         tail the CFL minimum of the new state is formed by the update pass itself; the
@@ -124,16 +150,21 @@ class HostPipeline:
 
     Every submitted state goes host -> device (pinned memory), takes one graph-captured
     level step and comes back device -> host. ``depth`` device slots (a LevelStepper each)
-    rotate so that the upload of submission k+1, the step of submission k and the download
-    of submission k-1 run at the same time: uploads and downloads use separate copy
-    streams (the two DMA directions are independent) and the steps share one compute
-    stream. Per submission the full state crosses the bus once each way.
+    rotate so that uploads, steps and downloads of successive submissions run at the same
+    time: uploads and downloads use separate copy streams (the two DMA directions are
+    independent) and the steps share one compute stream. A slot is reused only after its
+    previous result has left the device, so with the copies each longer than a step the
+    pipeline needs three slots to keep both DMA directions busy. With ``valid_only`` (the
+    default) only the valid rows cross the bus, each way (:meth:`LevelStepper.upload`,
+    :meth:`LevelStepper.download`; the step's ghost fill forms the ghost cells);
+    otherwise the whole state including ghost cells.
     """
 
-    def __init__(self, level, depth=2, **stepper_kw):
+    def __init__(self, level, depth=3, valid_only=True, **stepper_kw):
         import torch
 
         self.torch = torch
+        self.valid_only = bool(valid_only)
         self.slots = [LevelStepper(level, **stepper_kw) for _ in range(depth)]
         for s in self.slots:
             s.capture(fresh_dt=True)  # every submission is a new state
@@ -145,6 +176,8 @@ class HostPipeline:
         self.k = 0
         self.ncells = self.slots[0].ncells
         self.state_bytes = self.slots[0].state.data.numel() * 8
+        # bytes that cross the bus per submission, host to device and device to host
+        self.h2d_bytes = self.d2h_bytes = self.slots[0].row_bytes if self.valid_only else self.state_bytes
 
     def submit(self, host_in, host_out):
         """Enqueue one advance of ``host_in`` (pinned, the level's state shape) into
@@ -155,7 +188,10 @@ class HostPipeline:
         if self.used[b]:
             self.up.wait_event(self.ev_out[b])  # the slot's previous result has left the device
         with torch.cuda.stream(self.up):
-            slot.state.data.copy_(host_in, non_blocking=True)
+            if self.valid_only:
+                slot.upload(host_in, self.up)
+            else:
+                slot.state.data.copy_(host_in, non_blocking=True)
             self.ev_in[b].record(self.up)
         self.comp.wait_event(self.ev_in[b])
         with torch.cuda.stream(self.comp):
@@ -163,7 +199,10 @@ class HostPipeline:
             self.ev_step[b].record(self.comp)
         self.down.wait_event(self.ev_step[b])
         with torch.cuda.stream(self.down):
-            host_out.copy_(slot.state.data, non_blocking=True)
+            if self.valid_only:
+                slot.download(host_out, self.down)
+            else:
+                host_out.copy_(slot.state.data, non_blocking=True)
             self.ev_out[b].record(self.down)
         self.used[b] = True
         self.k += 1

@@ -63,6 +63,7 @@ SIGNATURES = {
     "pcg_estdt": ([C.c_int32, C.c_int32, _P(Box), C.c_double, _V, _V], C.c_int),
     "pcg_update_state": ([C.c_int32, C.c_int32, _P(Box), _A4, _V, _V], C.c_int),
     "pcg_fill_ghosts": ([_A4, _I3, _I3, _I3, C.c_int32, _V], C.c_int),
+    "pcg_copy_cells": ([_A4, _A4, _I3, _I3, _V], C.c_int),
     "pcg_plan_create": ([_PRM, C.c_int32, _P(Box), C.c_int32, _P(_V)], C.c_int),
     "pcg_plan_hydro": ([_V, _V, _V], C.c_int),
     "pcg_plan_stages": ([_V, C.c_int32, C.c_int32, _V, _V], C.c_int),

@@ -53,3 +53,23 @@ def test_unknown_boundary_types_are_rejected(bc):
     rc = _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), C.byref(abi.array4(u)),
              C.byref(abi.array4(o)), None, None)
     assert rc == -1
+
+
+def test_copy_cells_argument_errors():
+    """pcg_copy_cells rejects, before any device work, arrays that do not cover the box,
+    differing component counts and an empty box (PCG_EINVAL)."""
+    import numpy as np
+
+    a = abi.Fab(np.zeros((3, 6, 6, 6)), (0, 0, 0))
+    b = abi.Fab(np.zeros((2, 6, 6, 6)), (0, 0, 0))
+    c = abi.Fab(np.zeros((3, 4, 4, 4)), (1, 1, 1))
+
+    def rc(src, dst, lo, hi):
+        return _rc("pcg_copy_cells", C.byref(abi.array4(src)), C.byref(abi.array4(dst)), abi.ivec(lo), abi.ivec(hi),
+                   None)
+
+    assert rc(a, b, (0, 0, 0), (5, 5, 5)) == -1
+    assert "component counts" in native.load().pcg_last_error().decode()
+    assert rc(a, c, (0, 0, 0), (3, 3, 3)) == -1
+    assert "dst must cover" in native.load().pcg_last_error().decode()
+    assert rc(a, a, (2, 2, 2), (1, 5, 5)) == -1

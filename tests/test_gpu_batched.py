@@ -12,6 +12,8 @@ from particleclem_b200 import abi, hydro, workloads as wl
 from particleclem_b200.level import LevelStepper
 from test_oracle_golden import GOLDEN, load_case
 
+NG = abi.NGROW
+
 pytestmark = pytest.mark.gpu
 BIG = 1 << 30
 
@@ -182,28 +184,73 @@ def test_graph_replay_equals_eager_steps():
     b.close()
 
 
-def test_host_pipeline_equals_serial_steps():
+@pytest.mark.parametrize("depth,valid_only", [(2, False), (3, True)])
+def test_host_pipeline_equals_serial_steps(depth, valid_only):
     """Pipelined host->device->host advances equal one-at-a-time steps bit for bit, for
-    inputs that differ per submission and with more submissions than device slots."""
+    inputs that differ per submission and with more submissions than device slots; with
+    ``valid_only`` the valid rows cross the bus and the other ghost cells of the output
+    are left untouched."""
     import torch
 
     from particleclem_b200.level import HostPipeline
 
     levs = [wl.flame(n=16, box=8, seed=s) for s in (2, 3, 4)]
     ins = [torch.from_numpy(L.state).pin_memory() for L in levs]
+    if valid_only:  # the ghost cells of the inputs must not matter
+        for t in ins:
+            t[:, :NG] = -7.0
     order = [0, 1, 2, 1, 0, 2, 2]
-    outs = [torch.empty_like(ins[0]).pin_memory() for _ in order]
-    pipe = HostPipeline(levs[0], depth=2, precision=abi.PREC_MIXED, fuse=True)
+    outs = [torch.full_like(ins[0], 3.5).pin_memory() for _ in order]
+    pipe = HostPipeline(levs[0], depth=depth, valid_only=valid_only, precision=abi.PREC_MIXED, fuse=True)
     for i, j in enumerate(order):
         pipe.submit(ins[j], outs[i])
     pipe.synchronize()
     ref = LevelStepper(levs[0], precision=abi.PREC_MIXED, fuse=True)
     for i, j in enumerate(order):
-        ref.load_state(ins[j].to(ref.dev))
+        ref.load_state(torch.from_numpy(levs[j].state).to(ref.dev))
         ref.step()
-        np.testing.assert_array_equal(outs[i].numpy(), ref.host_state())
+        got, want = outs[i].numpy(), ref.host_state()
+        if valid_only:
+            rows = (slice(None), slice(NG, -NG), slice(NG, -NG), slice(None))
+            np.testing.assert_array_equal(got[rows], want[rows])
+            ghost = np.ones(got.shape, bool)
+            ghost[:, NG:-NG, NG:-NG, :] = False  # the valid rows, x ghost cells included
+            assert (got[ghost] == 3.5).all()
+        else:
+            np.testing.assert_array_equal(got, want)
     pipe.close()
     ref.close()
+
+
+@pytest.mark.parametrize("whole_rows", [False, True])
+def test_copy_cells_round_trip(whole_rows):
+    """pcg_copy_cells moves exactly the cells of the given box, host -> device -> host,
+    for FABs of different extents and origins (strided rows), and for boxes spanning
+    whole rows of both FABs (slices copied as contiguous runs)."""
+    import torch
+
+    from particleclem_b200 import hydro
+
+    rng = np.random.default_rng(3)
+    src = torch.from_numpy(rng.standard_normal((5, 9, 8, 7))).pin_memory()
+    if whole_rows:
+        dev = abi.Fab(torch.zeros((5, 12, 8, 7), dtype=torch.float64, device="cuda"), (0, 0, -2))
+        lo, hi = (0, 0, 1), (6, 7, 5)
+    else:
+        dev = abi.Fab(torch.zeros((5, 12, 11, 10), dtype=torch.float64, device="cuda"), (-3, -2, -1))
+        lo, hi = (1, 0, 2), (4, 5, 6)
+    back = torch.zeros((5, 9, 8, 7), dtype=torch.float64).pin_memory()
+    hydro.copy_cells(abi.Fab(src, (0, 0, 0)), dev, lo, hi)
+    hydro.copy_cells(dev, abi.Fab(back, (0, 0, 0)), lo, hi)
+    torch.cuda.synchronize()
+    sel = (slice(None), slice(lo[2], hi[2] + 1), slice(lo[1], hi[1] + 1), slice(lo[0], hi[0] + 1))
+    b = back.numpy()
+    np.testing.assert_array_equal(b[sel], src.numpy()[sel])
+    mask = np.ones(b.shape, bool)
+    mask[sel] = False
+    assert (b[mask] == 0).all()
+    d = dev.data.cpu().numpy()
+    assert np.count_nonzero(d) == np.count_nonzero(src.numpy()[sel])
 
 
 def test_mixed_level_step_error_vs_fp64():

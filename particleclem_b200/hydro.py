@@ -85,6 +85,7 @@ def make_box(lo, hi, uin, uout, dx, dt, domlo=None, domhi=None, bclo=(0, 0, 0), 
     if flx is not None:
         for d in range(3):
             b.flx[d] = abi.array4(flx[d])
+    b._keep = (uin, uout, flx)  # the descriptor holds raw pointers: keep the FABs alive with it
     return b
 
 

@@ -3,6 +3,7 @@
 Three translation units, all for sm_100a:
   pcg_kernels_strict.cu  FP64 kernels, --fmad=false (reference rounding, operation by operation)
   pcg_kernels_fast.cu    FP64 with FMA contraction, and the mixed FP32/FP64 kernels
+                         (FP32 division and square root approximate)
   pcg_host.cu            host runtime and the C ABI of include/pcg_hydro.h
 """
 from __future__ import annotations
@@ -24,7 +25,9 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
           "-I", SRC, "-I", os.path.join(ROOT, "include")]
 UNITS = {
     "pcg_kernels_strict.cu": ["--fmad=false"],
-    "pcg_kernels_fast.cu": ["--fmad=true"],
+    # FP32 division and square root as the hardware approximations (about 2 ulp): the
+    # mixed form's tolerance is 1e-6; FP64 arithmetic is not affected by these flags
+    "pcg_kernels_fast.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"],
     "pcg_host.cu": [],
 }
 

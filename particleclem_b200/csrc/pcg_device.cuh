@@ -261,7 +261,7 @@ struct Eos {
 template <class R> __device__ __forceinline__ R rdiv(R a, R b) { return a / b; }
 template <> __device__ __forceinline__ float rdiv<float>(float a, float b) { return __fdividef(a, b); }
 template <class R> __device__ __forceinline__ R rrcp(R a) { return R(1) / a; }
-template <> __device__ __forceinline__ float rrcp<float>(float a) { return __frcp_rn(a); }
+template <> __device__ __forceinline__ float rrcp<float>(float a) { return __fdividef(1.0f, a); }
 
 template <int NS, bool MIX, class R>
 struct EosR {

@@ -107,10 +107,49 @@ template <bool MIX> struct EosC<float, MIX> {
   static __device__ __forceinline__ const float* ec(int k, int r) { return e().ecf[k][r]; }
 };
 
+// Species sums of the FP32 mixture EOS with Blackwell's packed FP32 arithmetic (FFMA2,
+// two lanes per instruction): species 2m and 2m+1 share one instruction, their
+// coefficients one aligned pair of the species-minor rows (EosConst::cvp/ecp/imwp).
+// The even and odd species accumulate separately and meet at the end, so the order of
+// the additions differs from the scalar sums (well inside the mixed form's tolerance).
+__device__ __forceinline__ float2 cpair(const float* row, int k) { return *reinterpret_cast<const float2*>(row + k); }
+// sum_k y_k * P_k(t), P_k the degree NC-1 polynomial with coefficients rows[i][k]
+template <int NS, int NC>
+__device__ __forceinline__ float poly_sum_f2(float t, const float* y, const float (*rows)[pcg::MAXNS]) {
+  const float2 t2 = make_float2(t, t);
+  float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+  for (int m = 0; m < NS / 2; ++m) {
+    float2 c = cpair(rows[NC - 1], 2 * m);
+#pragma unroll
+    for (int i = NC - 2; i >= 0; --i) c = __ffma2_rn(t2, c, cpair(rows[i], 2 * m));
+    acc = __ffma2_rn(make_float2(y[2 * m], y[2 * m + 1]), c, acc);
+  }
+  float s = acc.x + acc.y;
+  if constexpr (NS % 2) {
+    float c = rows[NC - 1][NS - 1];
+#pragma unroll
+    for (int i = NC - 2; i >= 0; --i) c = fmaf(t, c, rows[i][NS - 1]);
+    s = fmaf(y[NS - 1], c, s);
+  }
+  return s;
+}
+// sum_k y_k * w[k]
+template <int NS>
+__device__ __forceinline__ float wsum_f2(const float* y, const float* w) {
+  float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+  for (int m = 0; m < NS / 2; ++m) acc = __ffma2_rn(make_float2(y[2 * m], y[2 * m + 1]), cpair(w, 2 * m), acc);
+  float s = acc.x + acc.y;
+  if constexpr (NS % 2) s = fmaf(y[NS - 1], w[NS - 1], s);
+  return s;
+}
+
 template <int NS, bool MIX, class R>
 struct Eos {
   using C = EosC<R, MIX>;
   static __device__ __forceinline__ R rmix(const R* y) {
+    if constexpr (sizeof(R) == 4 && NS > 1) return eos_ru<R>() * wsum_f2<NS>(y, C::e().imwp);
     R s = R(0);
 #pragma unroll
     for (int k = 0; k < NS; ++k) s = s + y[k] * C::imw(k);
@@ -139,6 +178,7 @@ struct Eos {
   // constant loads); the arithmetic is identical to the per-species selection.
   template <int RG>
   static __device__ __forceinline__ R cv_sum(R t, const R* y) {
+    if constexpr (sizeof(R) == 4 && NS > 1) return poly_sum_f2<NS, 5>(t, y, C::e().cvp[RG]);
     R cv = R(0);
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -149,6 +189,7 @@ struct Eos {
   }
   template <int RG>
   static __device__ __forceinline__ R e_sum(R t, const R* y) {
+    if constexpr (sizeof(R) == 4 && NS > 1) return poly_sum_f2<NS, 6>(t, y, C::e().ecp[RG]);
     R e = R(0);
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -268,6 +309,7 @@ struct EosR {
   using E = Eos<NS, MIX, R>;
   using C = EosC<R, MIX>;
   static __device__ __forceinline__ R sum_imw(const R* w) {
+    if constexpr (sizeof(R) == 4 && NS > 1) return wsum_f2<NS>(w, C::e().imwp);
     R s = R(0);
 #pragma unroll
     for (int k = 0; k < NS; ++k) s = s + w[k] * C::imw(k);

@@ -693,10 +693,10 @@ int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid, const dou
       c.ec[k][r][3] = rw * (a[2] / 3.0);
       c.ec[k][r][4] = rw * (a[3] / 4.0);
       c.ec[k][r][5] = rw * (a[4] / 5.0);
-      for (int i = 0; i < 5; ++i) c.cvcf[k][r][i] = (float)c.cvc[k][r][i];
-      for (int i = 0; i < 6; ++i) c.ecf[k][r][i] = (float)c.ec[k][r][i];
+      for (int i = 0; i < 5; ++i) c.cvcf[k][r][i] = c.cvp[r][i][k] = (float)c.cvc[k][r][i];
+      for (int i = 0; i < 6; ++i) c.ecf[k][r][i] = c.ecp[r][i][k] = (float)c.ec[k][r][i];
     }
-    c.imwf[k] = (float)c.imw[k];
+    c.imwf[k] = c.imwp[k] = (float)c.imw[k];
     c.tmidf[k] = (float)c.tmid[k];
   }
   return store_eos(1, c);

@@ -56,6 +56,11 @@ struct EosConst {
   float tmidf[MAXNS];
   float cvcf[MAXNS][2][5];
   float ecf[MAXNS][2][6];
+  // the same FP32 coefficients species-minor (zero past nspec), so that species 2m and
+  // 2m+1 form one aligned pair for the packed FP32 arithmetic (FFMA2)
+  alignas(8) float cvp[2][5][MAXNS];
+  alignas(8) float ecp[2][6][MAXNS];
+  alignas(8) float imwp[MAXNS];
 };
 
 // A strided block of memory addressed like amrex::Array4 (element type decided by the

@@ -145,6 +145,41 @@ __device__ __forceinline__ float wsum_f2(const float* y, const float* w) {
   return s;
 }
 
+// Species loops of the FP32 form in packed pairs: a[n] = ca * x[n] + cb * y[n] for
+// n < N (two species per FFMA2/FMUL2), returning the sum of the a[n].
+template <int N>
+__device__ __forceinline__ float blend2_sum(float ca, const float* x, float cb, const float* y, float* a) {
+  const float2 ca2 = make_float2(ca, ca), cb2 = make_float2(cb, cb);
+  float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+  for (int m = 0; m < N / 2; ++m) {
+    const float2 v = __ffma2_rn(ca2, make_float2(x[2 * m], x[2 * m + 1]),
+                                __fmul2_rn(cb2, make_float2(y[2 * m], y[2 * m + 1])));
+    a[2 * m] = v.x;
+    a[2 * m + 1] = v.y;
+    acc = __fadd2_rn(acc, v);
+  }
+  float s = acc.x + acc.y;
+  if constexpr (N % 2) {
+    a[N - 1] = fmaf(ca, x[N - 1], cb * y[N - 1]);
+    s += a[N - 1];
+  }
+  return s;
+}
+// a[n] = (r * q[n] - c[n]) * inv for n < N, in packed pairs
+template <int N>
+__device__ __forceinline__ void scale_sub2(float r, const float* q, const float* c, float inv, float* a) {
+  const float2 r2 = make_float2(r, r), i2 = make_float2(inv, inv);
+#pragma unroll
+  for (int m = 0; m < N / 2; ++m) {
+    const float2 v = __ffma2_rn(r2, make_float2(q[2 * m], q[2 * m + 1]), make_float2(-c[2 * m], -c[2 * m + 1]));
+    const float2 w = __fmul2_rn(v, i2);
+    a[2 * m] = w.x;
+    a[2 * m + 1] = w.y;
+  }
+  if constexpr (N % 2) a[N - 1] = fmaf(r, q[N - 1], -c[N - 1]) * inv;
+}
+
 template <int NS, bool MIX, class R>
 struct Eos {
   using C = EosC<R, MIX>;
@@ -622,10 +657,17 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
   po = mid ? R(0.5) * (pl + pr) : po;
   R rspo[NS];
   R ro = R(0);
+  if constexpr (sizeof(R) == 4 && NS > 1) {
+    // the upwind (or averaged) partial densities as al * yL + ar * yR, species in pairs
+    const R al = mid ? R(0.5) * rl : (mask ? rl : R(0));
+    const R ar = mid ? R(0.5) * rr : (mask ? R(0) : rr);
+    ro = blend2_sum<NS>(al, L.y, ar, Rs.y, rspo);
+  } else {
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    rspo[n] = mid ? R(0.5) * (rl * L.y[n] + rr * Rs.y[n]) : (mask ? rl * L.y[n] : rr * Rs.y[n]);
-    ro += rspo[n];
+    for (int n = 0; n < NS; n++) {
+      rspo[n] = mid ? R(0.5) * (rl * L.y[n] + rr * Rs.y[n]) : (mask ? rl * L.y[n] : rr * Rs.y[n]);
+      ro += rspo[n];
+    }
   }
   const R co = ER::cs_w(ro, pabs(po, p0), rspo);
   const R drho = rdiv(pstar - po, co * co);
@@ -659,10 +701,16 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
   const R qint_iu = use_star ? ustar : use_orig ? uo : frac * ustar + (R(1) - frac) * uo;
   const R qint_gdpres = use_star ? pstar : use_orig ? po : frac * pstar + (R(1) - frac) * po;
   R rgd = R(0);
+  if constexpr (sizeof(R) == 4 && NS > 1) {
+    const R cs = use_star ? R(1) : use_orig ? R(0) : frac;
+    const R cn = use_star ? R(0) : use_orig ? R(1) : R(1) - frac;
+    rgd = blend2_sum<NS>(cs, rspstar, cn, rspo, rspo);
+  } else {
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    rspo[n] = use_star ? rspstar[n] : use_orig ? rspo[n] : frac * rspstar[n] + (R(1) - frac) * rspo[n];
-    rgd += rspo[n];
+    for (int n = 0; n < NS; n++) {
+      rspo[n] = use_star ? rspstar[n] : use_orig ? rspo[n] : frac * rspstar[n] + (R(1) - frac) * rspo[n];
+      rgd += rspo[n];
+    }
   }
   const R regd = ER::rhoe_w(pabs(qint_gdpres, p0), rspo);
   const R frho = rgd * qint_iu;
@@ -836,10 +884,17 @@ __device__ __forceinline__ void cmpflx(const R* ql, const R* qr, int idx, int bc
   fl[pcg::UEDEN] = o.feden;
   fl[pcg::UEINT] = o.feint;
   const R flxrho = o.frho;
+  if constexpr (sizeof(R) == 4 && NS > 1) {
+    // pc_cmpflx_passive as ca * yL + cb * yR, species in pairs
+    const R ca = (o.ustar > R(0)) ? flxrho : (o.ustar < R(0)) ? R(0) : flxrho * R(0.5);
+    const R cb = (o.ustar > R(0)) ? R(0) : (o.ustar < R(0)) ? flxrho : flxrho * R(0.5);
+    blend2_sum<NS>(ca, ql + pcg::TR_Y, cb, qr + pcg::TR_Y, fl + pcg::UFS);
+  } else {
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    const R a = ql[pcg::TR_Y + n], b = qr[pcg::TR_Y + n];
-    fl[pcg::UFS + n] = (o.ustar > R(0)) ? flxrho * a : (o.ustar < R(0)) ? flxrho * b : flxrho * R(0.5) * (a + b);
+    for (int n = 0; n < NS; n++) {
+      const R a = ql[pcg::TR_Y + n], b = qr[pcg::TR_Y + n];
+      fl[pcg::UFS + n] = (o.ustar > R(0)) ? flxrho * a : (o.ustar < R(0)) ? flxrho * b : flxrho * R(0.5) * (a + b);
+    }
   }
   gun = o.gun;
   gpres = o.gpres;

@@ -699,11 +699,18 @@ __device__ __forceinline__ void transdo_apply(const R* qn, const KF& K, R p0, R*
   const R rr = qn[pcg::TR_RHO];
   const R rrnew = rr - flxrho;
   const R irrnew = EXACT ? R(0) : rrcp(rrnew);
+  if constexpr (sizeof(R) == 4 && NS > 1) {
+    R kc[NS];
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    const R compn = K(pcg::FL_Y + n);
-    const R compo = rr * qn[pcg::TR_Y + n] - compn;
-    out[pcg::TR_Y + n] = EXACT ? compo / rrnew : compo * irrnew;
+    for (int n = 0; n < NS; n++) kc[n] = K(pcg::FL_Y + n);
+    scale_sub2<NS>(rr, qn + pcg::TR_Y, kc, irrnew, out + pcg::TR_Y);
+  } else {
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+      const R compn = K(pcg::FL_Y + n);
+      const R compo = rr * qn[pcg::TR_Y + n] - compn;
+      out[pcg::TR_Y + n] = EXACT ? compo / rrnew : compo * irrnew;
+    }
   }
   R ru = qn[pcg::TR_U], rv = qn[pcg::TR_V], rw = qn[pcg::TR_W];
   const R ekin = R(0.5) * rr * (ru * ru + rv * rv + rw * rw);
@@ -970,12 +977,20 @@ __device__ __forceinline__ void transdd_apply(const R* qn, const R* K, R hdt, bo
   const R rr = qn[pcg::TR_RHO];
   const R rrnew = rr - flxrho;
   const R irrnew = EXACT ? R(0) : rrcp(rrnew);
+  if constexpr (sizeof(R) == 4 && NS > 1) {
+    scale_sub2<NS>(rr, qn + pcg::TR_Y, K + pcg::FL_Y, irrnew, out + pcg::TR_Y);
+    if (has_src) {
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    const R srcpass = has_src ? R(sq[pcg::QFS + n]) : R(0);
-    const R compn = K[pcg::FL_Y + n];
-    const R compo = rr * qn[pcg::TR_Y + n] - compn;
-    out[pcg::TR_Y + n] = (EXACT ? compo / rrnew : compo * irrnew) + hdt * srcpass;
+      for (int n = 0; n < NS; n++) out[pcg::TR_Y + n] += hdt * R(sq[pcg::QFS + n]);
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+      const R srcpass = has_src ? R(sq[pcg::QFS + n]) : R(0);
+      const R compn = K[pcg::FL_Y + n];
+      const R compo = rr * qn[pcg::TR_Y + n] - compn;
+      out[pcg::TR_Y + n] = (EXACT ? compo / rrnew : compo * irrnew) + hdt * srcpass;
+    }
   }
   const R pxnew = K[5 + NS];
   const R pynew = K[6 + NS];

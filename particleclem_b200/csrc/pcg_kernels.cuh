@@ -685,8 +685,24 @@ struct CorrArray {
 template <int NS, class R>
 __device__ __forceinline__ void transdo_corr(const CellPtr<const R>& f, int64_t ostride, R cdtdx, R c, R p0, R* K) {
   const TransdoCorr<NS, R> kc{f, shift(f, ostride), cdtdx, c, p0};
+  constexpr int NC = pcg::FL_Y + NS;
+  if constexpr (sizeof(R) == 4) {
+    // the flux differences in component pairs with packed FP32 (FMUL2)
+    const CellPtr<const R> g = kc.g;
+    const float2 c2 = make_float2(cdtdx, cdtdx);
 #pragma unroll
-  for (int n = 0; n < ncorr1<NS>(); ++n) K[n] = kc(n);
+    for (int m = 0; m < NC / 2; ++m) {
+      const int n = 2 * m;
+      const float2 v = __fmul2_rn(c2, __fadd2_rn(make_float2(g[n], g[n + 1]), make_float2(-f[n], -f[n + 1])));
+      K[n] = v.x;
+      K[n + 1] = v.y;
+    }
+    if constexpr (NC % 2) K[NC - 1] = kc(NC - 1);
+    K[NC] = kc(NC);
+  } else {
+#pragma unroll
+    for (int n = 0; n < ncorr1<NS>(); ++n) K[n] = kc(n);
+  }
 }
 
 template <int NS, bool EXACT, class R, class KF>
@@ -947,8 +963,24 @@ template <int NS, class R>
 __device__ __forceinline__ void transdd_corr(const CellPtr<const R>& fx, int64_t xst, const CellPtr<const R>& fy,
                                              int64_t yst, R cdtdx0, R cdtdx1, R c, R p0, R* K) {
   const CellPtr<const R> gx = shift(fx, xst), gy = shift(fy, yst);
+  constexpr int NC = pcg::FL_Y + NS;
+  if constexpr (sizeof(R) == 4) {
+    // component pairs with packed FP32 (FFMA2)
+    const float2 c0 = make_float2(cdtdx0, cdtdx0), c1 = make_float2(cdtdx1, cdtdx1);
 #pragma unroll
-  for (int n = 0; n < pcg::FL_Y + NS; ++n) K[n] = cdtdx0 * (gx[n] - fx[n]) + cdtdx1 * (gy[n] - fy[n]);
+    for (int m = 0; m < NC / 2; ++m) {
+      const int n = 2 * m;
+      const float2 dx = __fadd2_rn(make_float2(gx[n], gx[n + 1]), make_float2(-fx[n], -fx[n + 1]));
+      const float2 dy = __fadd2_rn(make_float2(gy[n], gy[n + 1]), make_float2(-fy[n], -fy[n + 1]));
+      const float2 v = __ffma2_rn(c0, dx, __fmul2_rn(c1, dy));
+      K[n] = v.x;
+      K[n + 1] = v.y;
+    }
+    if constexpr (NC % 2) K[NC - 1] = cdtdx0 * (gx[NC - 1] - fx[NC - 1]) + cdtdx1 * (gy[NC - 1] - fy[NC - 1]);
+  } else {
+#pragma unroll
+    for (int n = 0; n < NC; ++n) K[n] = cdtdx0 * (gx[n] - fx[n]) + cdtdx1 * (gy[n] - fy[n]);
+  }
   const int gp = pcg::FL_Y + NS, gu = pcg::FL_Y + NS + 1;
   const R dAupx = gx[gp] * gx[gu] - fx[gp] * fx[gu];
   const R pavx = R(0.5) * (gx[gp] + fx[gp]);

@@ -460,7 +460,7 @@ def run_ours(args):
                         "budget_gb": 120, "saturated_cell_updates_per_s": serving[0]["cell_updates_per_s"],
                         "loads": [{k: r[k] for k in ("load", "p50_ms", "p99_ms", "cell_updates_per_s", "batches")}
                                   for r in serving[1:]]},
-            "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 3, stages 6, fused tail 1, final dt 1
+            "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 1, stages 6, fused tail 1, final dt 1
             "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},
             "roofline": roof,

@@ -161,34 +161,50 @@ __global__ void __launch_bounds__(128, MINB) k_advance(pcg::StageArgs a) {
   if (threadIdx.x == 0) a.partial[blockIdx.x] = dtc;
 }
 
-// Single-level FillBoundary of one direction: the ghost slabs of a domain FAB that
-// covers grow(domain, ng), full extent in the other two directions (so corners are
-// filled consistently when the directions run x, y, z in turn).
+// Single-level FillBoundary of a domain FAB that covers grow(domain, ng), every ghost
+// cell in one pass. Filling the directions x, y, z in turn, each over the full extent of
+// the others (periodic wrap or foextrap, the zero-gradient copy of the nearest valid
+// layer), leaves in ghost cell (i, j, k) the valid cell (m_x(i), m_y(j), m_z(k)), with m_d
+// the wrap or clamp of direction d and the identity on valid indices; each thread copies
+// that cell directly. Threads cover the z ghost slabs (full x, y extent), then the y ghost
+// slabs of the valid k, then the x ghost slabs of the valid (j, k), i fastest.
+__device__ __forceinline__ int ghost_src(int c, int lo, int hi, bool periodic) {
+  const int n = hi - lo + 1;
+  if (c < lo) return periodic ? c + n : lo;
+  if (c > hi) return periodic ? c - n : hi;
+  return c;
+}
 __global__ void __launch_bounds__(128) k_fill(pcg::AuxArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int d = a.dir, ng = a.ng;
-  int ext[3];
-  for (int e = 0; e < 3; ++e) ext[e] = a.dhi[e] - a.dlo[e] + 1 + 2 * ng;
-  ext[d] = 2 * ng;  // ghost layers of direction d only
-  const int64_t ncell = (int64_t)ext[0] * ext[1] * ext[2];
-  if (t >= ncell) return;
+  const int ng = a.ng;
+  const int n0 = a.dhi[0] - a.dlo[0] + 1, n1 = a.dhi[1] - a.dlo[1] + 1, n2 = a.dhi[2] - a.dlo[2] + 1;
+  const int64_t e0 = n0 + 2 * ng, e1 = n1 + 2 * ng;
+  const int64_t cz = e0 * e1 * 2 * ng, cy = e0 * 2 * ng * n2, cx = (int64_t)2 * ng * n1 * n2;
   int c[3];
-  c[0] = (int)(t % ext[0]);
-  c[1] = (int)((t / ext[0]) % ext[1]);
-  c[2] = (int)(t / ((int64_t)ext[0] * ext[1]));
-  int dst[3], src[3];
-  for (int e = 0; e < 3; ++e) dst[e] = a.dlo[e] - ng + c[e];
-  const int n = a.dhi[d] - a.dlo[d] + 1;
-  const int g = c[d];  // 0..ng-1 low side, ng..2ng-1 high side
-  dst[d] = (g < ng) ? a.dlo[d] - ng + g : a.dhi[d] + 1 + (g - ng);
-  for (int e = 0; e < 3; ++e) src[e] = dst[e];
-  if (a.periodic) {
-    src[d] = (g < ng) ? dst[d] + n : dst[d] - n;
+  if (t < cz) {  // z ghost slabs: (i, j) over the grown extent, 2 ng layers
+    const int g = (int)(t / (e0 * e1));
+    c[0] = (int)(t % e0) + a.dlo[0] - ng;
+    c[1] = (int)((t / e0) % e1) + a.dlo[1] - ng;
+    c[2] = (g < ng) ? a.dlo[2] - ng + g : a.dhi[2] + 1 + (g - ng);
+  } else if (t < cz + cy) {  // y ghost slabs of the valid k
+    const int64_t u = t - cz;
+    const int g = (int)((u / e0) % (2 * ng));
+    c[0] = (int)(u % e0) + a.dlo[0] - ng;
+    c[1] = (g < ng) ? a.dlo[1] - ng + g : a.dhi[1] + 1 + (g - ng);
+    c[2] = (int)(u / (e0 * 2 * ng)) + a.dlo[2];
+  } else if (t < cz + cy + cx) {  // x ghost slabs of the valid (j, k)
+    const int64_t u = t - cz - cy;
+    const int g = (int)(u % (2 * ng));
+    c[0] = (g < ng) ? a.dlo[0] - ng + g : a.dhi[0] + 1 + (g - ng);
+    c[1] = (int)((u / (2 * ng)) % n1) + a.dlo[1];
+    c[2] = (int)(u / ((int64_t)2 * ng * n1)) + a.dlo[2];
   } else {
-    src[d] = (g < ng) ? a.dlo[d] : a.dhi[d];
+    return;
   }
+  int src[3];
+  for (int d = 0; d < 3; ++d) src[d] = ghost_src(c[d], a.dlo[d], a.dhi[d], (a.periodic >> d) & 1);
   const V4<double> s = v4<double>(a.state);
-  for (int comp = 0; comp < a.ncomp; ++comp) s(dst[0], dst[1], dst[2], comp) = s(src[0], src[1], src[2], comp);
+  for (int comp = 0; comp < a.ncomp; ++comp) s(c[0], c[1], c[2], comp) = s(src[0], src[1], src[2], comp);
 }
 
 template <int NS, bool MIX>

@@ -929,20 +929,16 @@ int pcg_fill_ghosts(const pcg_array4* state, const int32_t domlo[3], const int32
   for (int d = 0; d < 3; ++d)
     if (periodic[d] && dom.n(d) < ng) return fail(PCG_EINVAL, "periodic direction %d shorter than ng", d);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  for (int d = 0; d < 3 && ng > 0; ++d) {
-    pcg::AuxArgs a{};
-    a.dir = d;
-    a.state = view_of(state);
-    for (int e = 0; e < 3; ++e) { a.dlo[e] = domlo[e]; a.dhi[e] = domhi[e]; }
-    a.ng = ng;
-    a.periodic = periodic[d] ? 1 : 0;
-    a.ncomp = state->ncomp;
-    int64_t ncell = 2 * (int64_t)ng;
-    for (int e = 0; e < 3; ++e)
-      if (e != d) ncell *= dom.n(e) + 2 * ng;
-    cudaError_t e = pcg_strict::launch_aux(AUX_FILL, 1, a, (ncell + kThreads - 1) / kThreads, s);
-    if (e != cudaSuccess) return fail(PCG_ECUDA, "fill_ghosts: %s", cudaGetErrorString(e));
-  }
+  if (ng == 0) return PCG_OK;
+  pcg::AuxArgs a{};
+  a.state = view_of(state);
+  for (int e = 0; e < 3; ++e) { a.dlo[e] = domlo[e]; a.dhi[e] = domhi[e]; }
+  a.ng = ng;
+  a.periodic = (periodic[0] ? 1 : 0) | (periodic[1] ? 2 : 0) | (periodic[2] ? 4 : 0);
+  a.ncomp = state->ncomp;
+  const int64_t ncell = grow(dom, ng).cells() - dom.cells();  // every ghost cell, one thread each
+  cudaError_t e = pcg_strict::launch_aux(AUX_FILL, 1, a, (ncell + kThreads - 1) / kThreads, s);
+  if (e != cudaSuccess) return fail(PCG_ECUDA, "fill_ghosts: %s", cudaGetErrorString(e));
   return PCG_OK;
 }
 

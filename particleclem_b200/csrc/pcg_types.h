@@ -158,14 +158,14 @@ struct AuxArgs {
   const AuxBox* boxes;
   const Seg* segs;
   int32_t nseg;
-  int32_t dir;          // ghost fill: direction
   double* partial;      // timestep: one minimum per block
   int64_t npartial;
   double cfl;
   double* dt_out;       // timestep result (device)
   const double* dt_in;  // state update: device dt (nullptr: per-box dt)
   View state;           // ghost fill: domain FAB
-  int32_t dlo[3], dhi[3], ng, periodic, ncomp;
+  int32_t dlo[3], dhi[3], ng, ncomp;
+  int32_t periodic;     // ghost fill: bit d set when direction d is periodic
 };
 
 }  // namespace pcg

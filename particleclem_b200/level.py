@@ -114,8 +114,8 @@ class LevelStepper:
             self.dt.copy_(self.dt_next)
         self.plan.advance(self.cfl, self.dt, self.dt_next, stream)
 
-    # fill (3 directions), hydro stages (6), fused consup/update/CFL minimum, final minimum
-    launches_per_step = 3 + 6 + 1 + 1
+    # ghost fill (one pass), hydro stages (6), fused consup/update/CFL minimum, final minimum
+    launches_per_step = 1 + 6 + 1 + 1
 
     def capture(self, fresh_dt=False):
         """Capture one step as a CUDA graph (after one eager step that warms the library:

@@ -12,6 +12,11 @@ level (all of x and y, whole boxes in z) as one device FAB, and a step is
   3. CFL timestep of the slab, then the minimum over all ranks
   4. hydro advance of the slab's boxes (one fused region) and the update.
 
+With the fused step tail (the default) step 4 is pcg_plan_advance, whose update pass
+also forms the slab's CFL minimum of the new state, and step 3 reduces that minimum
+over the ranks: no separate timestep pass, except on the first step and after the state
+was replaced (load_state), where step 3 runs the CFL reduction of the slab first.
+
 Steps 1+pack, unpack+3a and 4 are CUDA graphs; the exchange and the reduction are NCCL
 point-to-point and all-reduce calls through torch.distributed (DistComm), or direct
 device copies between slabs held by one process (LocalComm, used to check the
@@ -47,7 +52,7 @@ def halo_planes(state, ng=NG):
 class SlabStepper:
     """The device side of one rank's slab (see the module docstring)."""
 
-    def __init__(self, slab, nranks, rank, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, device=0):
+    def __init__(self, slab, nranks, rank, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, device=0, fused_tail=True):
         import torch
 
         self.torch = torch
@@ -66,6 +71,9 @@ class SlabStepper:
         self.hsrc = abi.Fab(torch.zeros((self.nv, nz, ny, nx), dtype=torch.float64, device=self.dev),
                             (slab.domlo[0], slab.domlo[1], slab.k0))
         self.dt = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self.fused_tail = bool(fused_tail)
+        self.dt_next = torch.zeros(1, dtype=torch.float64, device=self.dev)  # slab CFL minimum of the new state
+        self._primed = False
         self.prm = abi.make_params(slab.dx, 0.0, self.ns, slab.domlo, slab.domhi, slab.bclo, slab.bchi,
                                    precision_mode=precision)
         boxes = [hydro.make_box(lo, hi, self.state, self.hsrc, slab.dx, 0.0, slab.domlo, slab.domhi, slab.bclo,
@@ -95,23 +103,41 @@ class SlabStepper:
         if self.up is not None:
             self.sbuf["up"].copy_(self.views["send_up"])
 
-    def unpack_and_estdt(self):
+    def _unpack(self):
         if self.down is not None:
             self.views["recv_down"].copy_(self.rbuf["down"])
         if self.up is not None:
             self.views["recv_up"].copy_(self.rbuf["up"])
-        self.plan.estdt(self.cfl, self.dt)
+
+    def unpack_and_estdt(self):
+        """Unpack the received ghost planes; the slab's CFL timestep into dt (its CFL
+        reduction, or with the fused tail the minimum the previous advance formed)."""
+        self._unpack()
+        if self.fused_tail and self._primed:
+            self.dt.copy_(self.dt_next)
+        else:
+            self.plan.estdt(self.cfl, self.dt)
 
     def advance(self):
-        self.plan.hydro(self.dt)
-        self.plan.update(self.dt)
+        if self.fused_tail:
+            self.plan.advance(self.cfl, self.dt, self.dt_next)
+        else:
+            self.plan.hydro(self.dt)
+            self.plan.update(self.dt)
+
+    def load_state(self, src, non_blocking=False):
+        """Replace the slab's state; the next step takes a fresh CFL reduction."""
+        self.state.data.copy_(src, non_blocking=non_blocking)
+        self._primed = False
 
     def capture(self):
-        """CUDA graphs of the three local phases. One eager pass warms the library first
-        (its exchange-free unpack would leave stale ghost planes, so the state and dt are
-        restored afterwards: capturing does not advance the slab)."""
+        """CUDA graphs of the local phases (the timestep phase twice: from the CFL
+        reduction and, with the fused tail, from the previous advance's minimum). One
+        eager pass warms the library first (its exchange-free unpack would leave stale
+        ghost planes, so the state and dt are restored afterwards: capturing does not
+        advance the slab)."""
         torch = self.torch
-        saved, saved_dt = self.state.data.clone(), self.dt.clone()
+        saved, saved_dt, primed = self.state.data.clone(), self.dt.clone(), self._primed
         s = torch.cuda.Stream(device=self.dev)
         s.wait_stream(torch.cuda.current_stream(self.dev))
         with torch.cuda.stream(s):
@@ -124,19 +150,28 @@ class SlabStepper:
         self.dt.copy_(saved_dt)
         torch.cuda.synchronize(self.dev)
         del saved
-        gs = []
-        for fn in (self.fill_and_pack, self.unpack_and_estdt, self.advance):
+        gs = {}
+        for key, fn, prime in ((0, self.fill_and_pack, None), ("fresh", self.unpack_and_estdt, False),
+                               ("primed", self.unpack_and_estdt, True), (2, self.advance, None)):
+            if prime is not None:
+                self._primed = prime
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
                 fn()
-            gs.append(g)
+            gs[key] = g
+        self._primed = primed
         self.graphs = gs
 
     def phase(self, i):
         if self.graphs:
-            self.graphs[i].replay()
+            if i == 1:
+                self.graphs["primed" if self.fused_tail and self._primed else "fresh"].replay()
+            else:
+                self.graphs[i].replay()
         else:
             (self.fill_and_pack, self.unpack_and_estdt, self.advance)[i]()
+        if i == 2 and self.fused_tail:
+            self._primed = True
 
     def close(self):
         self.graphs = None

@@ -51,3 +51,34 @@ def test_slab_graphs_equal_eager_mixed():
     np.testing.assert_array_equal(_slabs_valid(a), _slabs_valid(b))
     for s in a + b:
         s.close()
+
+
+@pytest.mark.parametrize("captured", [False, True])
+def test_slab_fused_tail_equals_separate_passes_fp64(captured):
+    """The fused step tail (the update pass forms each slab's CFL minimum, reduced over
+    the slabs before the next step) against the separate CFL, hydro and update passes,
+    bit for bit in the plain FP64 form; then a state loaded mid-run restarts from a fresh
+    CFL reduction in both."""
+    lev = wl.flame(n=16, box=8)
+    a = [SlabStepper(wl.split_level(lev, 2, r, 8), 2, r, precision=abi.PREC_FP64) for r in range(2)]
+    b = [SlabStepper(wl.split_level(lev, 2, r, 8), 2, r, precision=abi.PREC_FP64, fused_tail=False)
+         for r in range(2)]
+    if captured:
+        for s in a:
+            s.capture()
+    comm = LocalComm()
+    for _ in range(3):
+        step(a, comm)
+        step(b, comm)
+        assert float(a[0].dt.item()) == float(b[0].dt.item())
+    np.testing.assert_array_equal(_slabs_valid(a), _slabs_valid(b))
+    fresh = [s.state.data.clone() for s in b]
+    for s, f in zip(a, fresh):
+        s.load_state(f)
+    for _ in range(2):
+        step(a, comm)
+        step(b, comm)
+        assert float(a[0].dt.item()) == float(b[0].dt.item())
+    np.testing.assert_array_equal(_slabs_valid(a), _slabs_valid(b))
+    for s in a + b:
+        s.close()

@@ -89,3 +89,27 @@ def test_serving_sweep_respects_budget():
     assert [r["load"] for r in res] == ["saturated", 0.5]
     for r in res:
         assert r["requests"] == len(pids) and 0 < r["p50_ms"] <= r["p99_ms"] and r["peak_bytes"] <= budget
+
+
+def test_box_batch_fused_tail_equals_separate_passes_fp64():
+    """Three steps of an uneven batch with the fused step tail (the update pass forms
+    the batch's next CFL minimum) equal the separate CFL, hydro and update passes bit for
+    bit in the plain FP64 form, eager and graph-replayed."""
+    patches, eos = _patches(EDGES[:4], 150)
+    a = BoxBatch(patches, eos, precision=abi.PREC_FP64)
+    b = BoxBatch(patches, eos, precision=abi.PREC_FP64, fused_tail=False)
+    c = BoxBatch(patches, eos, precision=abi.PREC_FP64)
+    c.capture()  # one eager step before capturing
+    for k in range(3):
+        a.step()
+        b.step()
+        if k == 0:
+            continue
+        c.replay()
+        assert float(a.dt.item()) == float(b.dt.item())
+    for x, y in zip(a.states, b.states):
+        np.testing.assert_array_equal(x.data.cpu().numpy(), y.data.cpu().numpy())
+    for x, y in zip(a.states, c.states):
+        np.testing.assert_array_equal(x.data.cpu().numpy(), y.data.cpu().numpy())
+    for s in (a, b, c):
+        s.close()

@@ -205,7 +205,9 @@ __device__ __forceinline__ double divu_node(const V4<const double>& q, int i, in
 }
 
 // prep components: 0 = flattening (min over the 3 directions, Source/PPM.cpp:108-115),
-// 1 = sound speed the trace uses (PPM: RPY2Cs, Source/PPM.cpp:101; PLM: qaux QC).
+// 1 = sound speed the trace uses (PPM: RPY2Cs, Source/PPM.cpp:101; PLM: qaux QC). The
+// flattening is evaluated in the compute type R: FP64 in the FP64 forms, FP32 in the
+// mixed form (the primitive values rounded to FP32; it departs from 1 only at shocks).
 template <int NS, bool MIX, bool EXACT, class R>
 __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
   Item it;
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
   R flat = R(1);
   if (a.use_flattening) {
 #pragma unroll
-    for (int df = 0; df < 3; df++) flat = dmin(flat, R(flatten<double>(q, i, j, k, df)));
+    for (int df = 0; df < 3; df++) flat = dmin(flat, flatten<R>(q, i, j, k, df));
   }
   R cc;
   if (a.ppm_type == 1) {

@@ -545,9 +545,10 @@ template <class R>
 __device__ __forceinline__ R ppm_s6(R sm, R sp, R sc) { return R(6) * sc - R(3) * (sm + sp); }
 
 // Source/Godunov.H:188-260 (flatten); the stencil +-3 lies inside the q FAB for every
-// cell the path traces (the q FAB covers grow(box,4), traced cells grow(box,1)).
-template <class R>
-__device__ __forceinline__ R flatten(const V4<const double>& q, int i, int j, int k, int dir) {
+// cell the path traces (the q FAB covers grow(box,4), traced cells grow(box,1)). q is any
+// accessor q(i, j, k, qcomp) of the primitive state.
+template <class R, class Q>
+__device__ __forceinline__ R flatten(const Q& q, int i, int j, int k, int dir) {
   const int di = dir == 0, dj = dir == 1, dk = dir == 2;
 #define QS(s, n) R(q(i + (s) * di, j + (s) * dj, k + (s) * dk, n))
   const int n = pcg::QPRES;

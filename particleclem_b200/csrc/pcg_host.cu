@@ -309,7 +309,8 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
     R.zero_uout = B.zero_uout ? 1 : 0;
     const IBox g4 = grow(B.bx, 4), g1 = grow(B.bx, 1);
     if (B.internal_q) {
-      take(L, g4, nq, 8, R.q);
+      // the mixed form keeps no FP64 primitive array: its stages read the FP32 copy
+      if (!single) take(L, g4, nq, 8, R.q);
       take(L, g4, pcg::NQAUX, 8, R.qa);
       add_seg(L, K_CTOPRIM, (int)r, 0, g4);
     } else {
@@ -320,8 +321,10 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
     if (single) {
       // mixed form: the FP32 primitive copy the trace reads, written by k_ctoprim, or by
       // k_prep when the caller supplies q (pcg_umdrv)
-      take(L, grow(B.bx, qf_grow), nt, 4, R.qf);
-      R.qf_grow = qf_grow;
+      // prep's flattening reads +-3 cells around grow(box,1) from this copy when ctoprim
+      // wrote it, so it covers grow(box,4) then
+      R.qf_grow = B.internal_q ? 4 : qf_grow;
+      take(L, grow(B.bx, R.qf_grow), nt, 4, R.qf);
       R.qf_in_prep = B.internal_q ? 0 : 1;
       add_seg(L, K_PREP, (int)r, 0, B.internal_q ? g1 : grow(B.bx, qf_grow));
     } else {
@@ -393,7 +396,10 @@ void rebase_workspace(Layout& L, const std::vector<BoxIn>& boxes, char* base) {
   for (size_t r = 0; r < L.regions.size(); ++r) {
     pcg::Region& R = L.regions[r];
     const BoxIn& B = boxes[r];
-    if (B.internal_q) { rebase(R.q, base); rebase(R.qa, base); }
+    if (B.internal_q) {
+      if (L.esz != 4) rebase(R.q, base);  // FP64 forms only (see build_layout)
+      rebase(R.qa, base);
+    }
     rebase(R.prep, base);
     if (R.qf.p || L.esz == 4) rebase(R.qf, base);
     rebase(R.divu, base);

@@ -131,7 +131,6 @@ __global__ void __launch_bounds__(128, MINB) k_ctoprim(pcg::StageArgs a) {
   const pcg::Region& rg = *it.rg;
   using E = Eos<NS, MIX, double>;
   const CellPtr<const double> u = at(v4<const double>(rg.uin), it.i, it.j, it.k);
-  const CellPtr<double> q = at(v4<double>(rg.q), it.i, it.j, it.k);
   const CellPtr<double> qa = at(v4<double>(rg.qa), it.i, it.j, it.k);
   const double rho = u[pcg::URHO];
   const double rhoinv = 1.0 / rho;
@@ -139,27 +138,33 @@ __global__ void __launch_bounds__(128, MINB) k_ctoprim(pcg::StageArgs a) {
   const double vy = u[pcg::UMY] * rhoinv;
   const double vz = u[pcg::UMZ] * rhoinv;
   const double kineng = 0.5 * rho * (vx * vx + vy * vy + vz * vz) - 0.5 * rho * 0.0 * 0.0 * 0.0 * 0.0;
-  q[pcg::QRHO] = rho;
-  q[pcg::QU] = vx;
-  q[pcg::QV] = vy;
-  q[pcg::QW] = vz;
   double y[NS];
 #pragma unroll
   for (int n = 0; n < NS; n++) {
     double yn = u[pcg::UFS + n] / rho;
     if ((-1e-4 * DBL_EPSILON < yn) && (yn < 1e-4 * DBL_EPSILON)) yn = 0.0;
     y[n] = yn;
-    q[pcg::QFS + n] = yn;
   }
   const double e = (u[pcg::UEDEN] - kineng) * rhoinv;
   const double wbar = E::y2wbar(y);
   const double T = E::rey2t(e, y, u[pcg::UTEMP]);
   double p, cs, gam1, dpde, dpdr_e;
   E::rty2all(rho, T, y, p, cs, gam1, dpde, dpdr_e);
-  q[pcg::QTEMP] = T;
-  q[pcg::QREINT] = e * rho;
-  q[pcg::QPRES] = p;
-  q[pcg::QGAME] = p / (e * rho) + 1.0;
+  // the FP64 primitive array exists in the FP64 forms; the mixed form's stages read the
+  // FP32 copy below instead
+  if (rg.q.p) {
+    const CellPtr<double> q = at(v4<double>(rg.q), it.i, it.j, it.k);
+    q[pcg::QRHO] = rho;
+    q[pcg::QU] = vx;
+    q[pcg::QV] = vy;
+    q[pcg::QW] = vz;
+#pragma unroll
+    for (int n = 0; n < NS; n++) q[pcg::QFS + n] = y[n];
+    q[pcg::QTEMP] = T;
+    q[pcg::QREINT] = e * rho;
+    q[pcg::QPRES] = p;
+    q[pcg::QGAME] = p / (e * rho) + 1.0;
+  }
   qa[pcg::QDPDR] = dpdr_e;
   qa[pcg::QDPDE] = dpde;
   qa[pcg::QGAMC] = gam1;
@@ -184,8 +189,32 @@ __global__ void __launch_bounds__(128, MINB) k_ctoprim(pcg::StageArgs a) {
 }
 
 // ------------------------------------------------------------------ prep
-// Source/Hydro.H:476-517 (pc_divu) at node (i,j,k)
-__device__ __forceinline__ double divu_node(const V4<const double>& q, int i, int j, int k, const double* dx) {
+// The component of the trace-state layout (FP32 primitive copy) holding QVAR component
+// qcomp.
+__device__ __forceinline__ int tr_comp(int qcomp) {
+  return qcomp == pcg::QRHO ? pcg::TR_RHO
+         : qcomp <= pcg::QW ? pcg::TR_U + (qcomp - pcg::QU)
+         : qcomp == pcg::QPRES ? pcg::TR_P
+         : qcomp == pcg::QREINT ? pcg::TR_RE
+                                : pcg::TR_Y + (qcomp - pcg::QFS);
+}
+
+// Primitive component qcomp of cell (i,j,k) read from the FP32 copy qf (trace-state
+// layout), the pressure back to absolute (deviation + p0), as type T: what prep reads in
+// the mixed form, where ctoprim writes no FP64 primitive array.
+template <class T>
+struct QfPrim {
+  V4<const float> f;
+  float p0;
+  __device__ __forceinline__ T operator()(int i, int j, int k, int qcomp) const {
+    const float v = f(i, j, k, tr_comp(qcomp));
+    return qcomp == pcg::QPRES ? T(v) + T(p0) : T(v);
+  }
+};
+
+// Source/Hydro.H:476-517 (pc_divu) at node (i,j,k); q any accessor of the primitives
+template <class Q>
+__device__ __forceinline__ double divu_node(const Q& q, int i, int j, int k, const double* dx) {
   const double ux = 0.25 *
                     (q(i, j, k, pcg::QU) - q(i - 1, j, k, pcg::QU) + q(i, j, k - 1, pcg::QU) -
                      q(i - 1, j, k - 1, pcg::QU) + q(i, j - 1, k, pcg::QU) - q(i - 1, j - 1, k, pcg::QU) +
@@ -202,6 +231,33 @@ __device__ __forceinline__ double divu_node(const V4<const double>& q, int i, in
                      q(i - 1, j - 1, k, pcg::QW) - q(i - 1, j - 1, k - 1, pcg::QW)) /
                     dx[2];
   return ux + vy + wz;
+}
+
+// Flattening, the trace's sound speed and the nodal div u of one cell of grow(box,1):
+// q is the accessor the flattening and the sound speed read, qd the one div u reads.
+template <int NS, bool MIX, bool EXACT, class R, class Q, class QD>
+__device__ __forceinline__ void prep_cell(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k,
+                                          const Q& q, const QD& qd) {
+  R flat = R(1);
+  if (a.use_flattening) {
+#pragma unroll
+    for (int df = 0; df < 3; df++) flat = dmin(flat, flatten<R>(q, i, j, k, df));
+  }
+  R cc;
+  if (a.ppm_type == 1) {
+    R y[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) y[n] = R(q(i, j, k, pcg::QFS + n));
+    const R rho = R(q(i, j, k, pcg::QRHO)), p = R(q(i, j, k, pcg::QPRES));
+    cc = EXACT ? Eos<NS, MIX, R>::rpy2cs(rho, p, y) : EosR<NS, MIX, R>::cs_y(rho, p, y);
+  } else {
+    cc = R(v4<const double>(rg.qa)(i, j, k, pcg::QC));
+  }
+  const CellPtr<R> pr = at(v4<R>(rg.prep), i, j, k);
+  pr[0] = flat;
+  pr[1] = cc;
+  if (i >= rg.lo[0] && i <= rg.hi[0] + 1 && j >= rg.lo[1] && j <= rg.hi[1] + 1 && k >= rg.lo[2] && k <= rg.hi[2] + 1)
+    v4<double>(rg.divu)(i, j, k) = divu_node(qd, i, j, k, rg.dx);
 }
 
 // prep components: 0 = flattening (min over the 3 directions, Source/PPM.cpp:108-115),
@@ -233,39 +289,21 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
   const bool in_g1 = i >= rg.lo[0] - 1 && i <= rg.hi[0] + 1 && j >= rg.lo[1] - 1 && j <= rg.hi[1] + 1 &&
                      k >= rg.lo[2] - 1 && k <= rg.hi[2] + 1;
   if (!in_g1) return;
-  R flat = R(1);
-  if (a.use_flattening) {
-#pragma unroll
-    for (int df = 0; df < 3; df++) flat = dmin(flat, flatten<R>(q, i, j, k, df));
+  if constexpr (PDev<R>::on) {
+    if (!rg.q.p) {  // mixed form after ctoprim: only the FP32 copy exists
+      const V4<const float> f = v4<const float>(rg.qf);
+      const float p0 = float(p0_of<NS, MIX, R>(rg));
+      prep_cell<NS, MIX, EXACT, R>(a, rg, i, j, k, QfPrim<R>{f, p0}, QfPrim<double>{f, p0});
+      return;
+    }
   }
-  R cc;
-  if (a.ppm_type == 1) {
-    R y[NS];
-#pragma unroll
-    for (int n = 0; n < NS; ++n) y[n] = R(q(i, j, k, pcg::QFS + n));
-    const R rho = R(q(i, j, k, pcg::QRHO)), p = R(q(i, j, k, pcg::QPRES));
-    cc = EXACT ? Eos<NS, MIX, R>::rpy2cs(rho, p, y) : EosR<NS, MIX, R>::cs_y(rho, p, y);
-  } else {
-    cc = R(v4<const double>(rg.qa)(i, j, k, pcg::QC));
-  }
-  const CellPtr<R> pr = at(v4<R>(rg.prep), i, j, k);
-  pr[0] = flat;
-  pr[1] = cc;
-  if (i >= rg.lo[0] && i <= rg.hi[0] + 1 && j >= rg.lo[1] && j <= rg.hi[1] + 1 && k >= rg.lo[2] && k <= rg.hi[2] + 1)
-    v4<double>(rg.divu)(i, j, k) = divu_node(q, i, j, k, rg.dx);
+  prep_cell<NS, MIX, EXACT, R>(a, rg, i, j, k, q, q);
 }
 
 // ------------------------------------------------------------------ trace
 // The primitive state the trace reads: q itself (double, QVAR layout) in the FP64
 // forms; in the mixed form the FP32 copy qf written by k_prep (trace-state layout,
 // pressure as the deviation from the box's p0), so no conversions are left in the trace.
-__device__ __forceinline__ int tr_comp(int qcomp) {
-  return qcomp == pcg::QRHO ? pcg::TR_RHO
-         : qcomp <= pcg::QW ? pcg::TR_U + (qcomp - pcg::QU)
-         : qcomp == pcg::QPRES ? pcg::TR_P
-         : qcomp == pcg::QREINT ? pcg::TR_RE
-                                : pcg::TR_Y + (qcomp - pcg::QFS);
-}
 template <class R> struct Prim;
 template <> struct Prim<double> {
   const double* p;

@@ -72,9 +72,10 @@ class HydroParams(C.Structure):
 
 
 def make_params(dx, dt, nspec, domlo, domhi, bclo, bchi, ppm_type=1, plm_iorder=4,
-                use_flattening=True, difmag=0.1, precision_mode=PREC_FP64) -> HydroParams:
+                use_flattening=True, difmag=0.1, precision_mode=PREC_FP64, use_hybrid_weno=False,
+                weno_scheme=1) -> HydroParams:
     """Parameter block with PeleC's defaults (Source/Params/_cpp_parameters: difmag 0.1,
-    plm_iorder 4, use_flattening true; hybrid WENO off)."""
+    plm_iorder 4, use_flattening true; hybrid WENO off, weno_scheme 1)."""
     p = HydroParams()
     p.dx[:] = [float(v) for v in dx]
     p.dt = float(dt)
@@ -82,8 +83,8 @@ def make_params(dx, dt, nspec, domlo, domhi, bclo, bchi, ppm_type=1, plm_iorder=
     p.ppm_type = int(ppm_type)
     p.plm_iorder = int(plm_iorder)
     p.use_flattening = int(bool(use_flattening))
-    p.use_hybrid_weno = 0
-    p.weno_scheme = 1
+    p.use_hybrid_weno = int(bool(use_hybrid_weno))
+    p.weno_scheme = int(weno_scheme)
     p.domlo[:] = [int(v) for v in domlo]
     p.domhi[:] = [int(v) for v in domhi]
     p.bclo[:] = [int(v) for v in bclo]

@@ -27,7 +27,7 @@ class _nullctx:
 
 class LevelStepper:
     def __init__(self, level, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, ppm_type=1, plm_iorder=4,
-                 use_flattening=True, difmag=0.1, device=0, fused_tail=True):
+                 use_flattening=True, difmag=0.1, device=0, fused_tail=True, use_hybrid_weno=False, weno_scheme=1):
         import torch
 
         self.torch = torch
@@ -49,7 +49,8 @@ class LevelStepper:
         self._primed = False
         self.prm = abi.make_params(level.dx, 0.0, self.ns, level.domlo, level.domhi, level.bclo, level.bchi,
                                    ppm_type=ppm_type, plm_iorder=plm_iorder, use_flattening=use_flattening,
-                                   difmag=difmag, precision_mode=precision)
+                                   difmag=difmag, precision_mode=precision, use_hybrid_weno=use_hybrid_weno,
+                                   weno_scheme=weno_scheme)
         self.boxes = [hydro.make_box(lo, hi, self.state, self.hsrc, level.dx, 0.0, level.domlo, level.domhi,
                                      level.bclo, level.bchi) for lo, hi in level.boxes]
         self.plan = hydro.Plan(self.prm, self.boxes, fuse=fuse)

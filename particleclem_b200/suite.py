@@ -2,11 +2,15 @@
 
   python -m particleclem_b200.suite batch   512 independent flame boxes, edges log-uniform
                                             in [8, 64] per axis (9 species): one batched step
-                                            (13 launches, CUDA graph), mixed and plain FP64,
+                                            (CUDA graph), mixed and plain FP64,
                                             per-component error of mixed against FP64
   python -m particleclem_b200.suite sweep   256^3 periodic turbulence in 64 boxes of 64^3
                                             (gamma law): PPM and PLM x {FP64, mixed}, error
                                             growth of mixed against FP64 over the steps
+  python -m particleclem_b200.suite options the headline flame level with each reconstruction
+                                            option (PPM, hybrid WENO-JS5/Z5/Z7/Z3) and with
+                                            an inflow low-z face (low-order boundary fluxes):
+                                            FP64 and mixed step times, mixed error
   python -m particleclem_b200.suite serve   16 ensemble runs submitting flame boxes with
                                             edges in {16,24,32,48,64}: saturated throughput
                                             and p50/p99 latency under Poisson arrivals at
@@ -182,6 +186,41 @@ def run_serve(args):
                                                       "hydro_source_max_rel_l1": worst_src}}), flush=True)
 
 
+def run_options(args):
+    """The 128^3 flame level step (FP64 per box as the drop-in, mixed fused, CUDA graphs)
+    with the reference's remaining reconstruction and boundary options."""
+    import torch
+
+    from .level import LevelStepper
+
+    cases = [("ppm", {}, False)] + [
+        (f"hybrid_weno_{n}", {"use_hybrid_weno": True, "weno_scheme": s}, False)
+        for s, n in ((0, "js5"), (1, "z5"), (2, "z7"), (3, "z3"))] + [("ppm_inflow_zlo", {}, True)]
+    g = abi.NGROW
+    for name, kw, inflow in cases:
+        lev = wl.flame(n=args.n, box=args.box, seed=2)
+        if inflow:
+            lev.bclo = (lev.bclo[0], lev.bclo[1], abi.BC_INFLOW)
+        ms, states = {}, {}
+        for form, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+            st = LevelStepper(lev, precision=prec, fuse=prec == abi.PREC_MIXED, **kw)
+            st.step()  # one step from the generated state, kept for the error
+            torch.cuda.synchronize()
+            states[form] = st.state.data[:, g:-g, g:-g, g:-g].clone()
+            st.capture()
+            ms[form] = _timed(torch, st.replay, args.steps, args.warmup)
+            st.close()
+            del st
+            torch.cuda.empty_cache()
+        l1, li = _rel(torch, states["fp64"], states["mixed"])
+        print(json.dumps({"workload": f"flame_level_{args.n}^3_{name}", "fp64_ms_per_step": ms["fp64"],
+                          "mixed_ms_per_step": ms["mixed"], "speedup_mixed_over_fp64": ms["fp64"] / ms["mixed"],
+                          "mixed_cell_updates_per_s": lev.ncells() / (ms["mixed"] / 1e3),
+                          "error_mixed_vs_fp64_one_step": {"max_rel_l1": float(l1.max()),
+                                                           "max_rel_linf": float(li.max())}}), flush=True)
+        del states
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -200,8 +239,13 @@ def main(argv=None):
     v.add_argument("--budget-gb", type=float, default=120.0)
     v.add_argument("--loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.9, 1.0])
     v.add_argument("--error-sample", type=int, default=32)
+    o = sub.add_parser("options")
+    o.add_argument("--n", type=int, default=128)
+    o.add_argument("--box", type=int, default=32)
+    o.add_argument("--steps", type=int, default=10)
+    o.add_argument("--warmup", type=int, default=3)
     args = ap.parse_args(argv)
-    {"batch": run_batch, "sweep": run_sweep, "serve": run_serve}[args.cmd](args)
+    {"batch": run_batch, "sweep": run_sweep, "serve": run_serve, "options": run_options}[args.cmd](args)
     return 0
 
 

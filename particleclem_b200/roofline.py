@@ -21,7 +21,7 @@ re-reads). For a region of valid edges (nx, ny, nz), NS species, compute-type si
            values per face of the box (FP32 in the mixed form without flux export)
 * consup:  read 3 (NVAR + 2) final-flux values per face, write NVAR doubles per cell
 
-The path-level figure is the survey's B_alg = 8 NVAR [(nx+8)(ny+8)(nz+8) + nx ny nz]
+The path-level figure is B_alg = 8 NVAR [(nx+8)(ny+8)(nz+8) + nx ny nz]
 bytes per box (read the grown state once, write the hydro source once).
 """
 from __future__ import annotations

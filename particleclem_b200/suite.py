@@ -9,8 +9,9 @@
                                             growth of mixed against FP64 over the steps
   python -m particleclem_b200.suite options the headline flame level with each reconstruction
                                             option (PPM, hybrid WENO-JS5/Z5/Z7/Z3) and with
-                                            an inflow low-z face (low-order boundary fluxes):
-                                            FP64 and mixed step times, mixed error
+                                            an inflow low-z face (low-order boundary fluxes),
+                                            and the 32^3 Sod box: FP64 and mixed step times,
+                                            mixed error
   python -m particleclem_b200.suite serve   16 ensemble runs submitting flame boxes with
                                             edges in {16,24,32,48,64}: saturated throughput
                                             and p50/p99 latency under Poisson arrivals at
@@ -188,17 +189,20 @@ def run_serve(args):
 
 def run_options(args):
     """The 128^3 flame level step (FP64 per box as the drop-in, mixed fused, CUDA graphs)
-    with the reference's remaining reconstruction and boundary options."""
+    with the reference's remaining reconstruction and boundary options, and the single
+    32^3 Sod box (one species) the same way."""
     import torch
 
     from .level import LevelStepper
 
-    cases = [("ppm", {}, False)] + [
-        (f"hybrid_weno_{n}", {"use_hybrid_weno": True, "weno_scheme": s}, False)
-        for s, n in ((0, "js5"), (1, "z5"), (2, "z7"), (3, "z3"))] + [("ppm_inflow_zlo", {}, True)]
+    flame = f"flame_level_{args.n}^3_"
+    cases = [(flame + "ppm", {}, False)] + [
+        (flame + f"hybrid_weno_{n}", {"use_hybrid_weno": True, "weno_scheme": s}, False)
+        for s, n in ((0, "js5"), (1, "z5"), (2, "z7"), (3, "z3"))] + [(flame + "ppm_inflow_zlo", {}, True),
+                                                                      ("sod_32^3_one_box_ppm", {}, None)]
     g = abi.NGROW
     for name, kw, inflow in cases:
-        lev = wl.flame(n=args.n, box=args.box, seed=2)
+        lev = wl.sod(n=32) if inflow is None else wl.flame(n=args.n, box=args.box, seed=2)
         if inflow:
             lev.bclo = (lev.bclo[0], lev.bclo[1], abi.BC_INFLOW)
         ms, states = {}, {}
@@ -213,7 +217,7 @@ def run_options(args):
             del st
             torch.cuda.empty_cache()
         l1, li = _rel(torch, states["fp64"], states["mixed"])
-        print(json.dumps({"workload": f"flame_level_{args.n}^3_{name}", "fp64_ms_per_step": ms["fp64"],
+        print(json.dumps({"workload": name, "fp64_ms_per_step": ms["fp64"],
                           "mixed_ms_per_step": ms["mixed"], "speedup_mixed_over_fp64": ms["fp64"] / ms["mixed"],
                           "mixed_cell_updates_per_s": lev.ncells() / (ms["mixed"] / 1e3),
                           "error_mixed_vs_fp64_one_step": {"max_rel_l1": float(l1.max()),

@@ -647,8 +647,12 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
   const R wl = dmax(wsmall, cl * rl);
   const R wr = dmax(wsmall, cr * rr);
   const R iwlr = rrcp(wl + wr);
-  const R pstar = dmax(pfloor(Lim<R>::tiny(), p0), ((wr * pl + wl * pr) + wl * wr * (ul - ur)) * iwlr);
-  R ustar = ((wl * ul + wr * ur) + (pl - pr)) * iwlr;
+  // the star state as the left state plus weighted jumps: (wr pl + wl pr + wl wr (ul - ur))
+  // / (wl + wr) and (wl ul + wr ur + pl - pr) / (wl + wr) rearranged, so that equal left and
+  // right pressures (velocities) give exactly that pressure (velocity) without FP32
+  // rounding noise in uniform regions
+  const R pstar = dmax(pfloor(Lim<R>::tiny(), p0), pl + (wl * (pr - pl) + wl * wr * (ul - ur)) * iwlr);
+  R ustar = ul + (wr * (ur - ul) + (pl - pr)) * iwlr;
   bool mask = ustar > R(0);
   R uo = mask ? ul : ur;
   R po = mask ? pl : pr;

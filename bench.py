@@ -192,9 +192,9 @@ def run_cpu_configs(args):
     for name, make, ppm in cases:
         arm = CpuArm(make(), ppm_type=ppm)
         arm.measure(min(2.0, args.cpu_seconds))  # warm
-        vals = [arm.measure(args.cpu_seconds / 3) for _ in range(3)]
+        vals = [arm.measure(args.cpu_seconds / 5) for _ in range(5)]
         vals.sort(key=lambda r: r["value"])
-        med = vals[1]
+        med = vals[2]  # median of five samples
         print(json.dumps({"config": {"workload": name}, "cpu_baseline": med,
                           "runs": [round(r["value"]) for r in vals]}), flush=True)
         arm.pool.shutdown()

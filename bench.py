@@ -236,7 +236,7 @@ def run_ours(args):
     # 4-cell halo exchange (NCCL send/recv) and the dt all-reduce-min every step.
     if world == 1:
         lev = wl.flame(n=args.n, box=args.box, seed=2)
-        st = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True)
+        st = LevelStepper(lev, precision=abi.PREC_MIXED, fuse=True, device=local)
         st.step()  # valid dt and intermediates for the launch-shape autotuner
         tuned = {"mixed": autotune.tune(st.plan, st.dt, reps=3, state=st.state.data)}
         st.capture()
@@ -246,7 +246,7 @@ def run_ours(args):
         from particleclem_b200.slab import DistComm, SlabStepper, step as slab_step
 
         slab = wl.flame_slab(n=args.n, nz=args.n * world, nranks=world, rank=rank, box=args.box, seed=2)
-        st = SlabStepper(slab, world, rank, precision=abi.PREC_MIXED, fuse=True)
+        st = SlabStepper(slab, world, rank, precision=abi.PREC_MIXED, fuse=True, device=local)
         st.fill()
         st.plan.estdt(st.cfl, st.dt)  # a local dt for the launch-shape autotuner
         tuned = {"mixed": autotune.tune(st.plan, st.dt, reps=3, state=st.state.data)}
@@ -322,7 +322,7 @@ def run_ours(args):
 
     # ---- plain FP64 drop-in: per-box (reference) semantics, reference operation order
     lev64 = wl.flame(n=args.n, box=args.box, seed=2 + rank)
-    st64 = LevelStepper(lev64, precision=abi.PREC_FP64, fuse=False)
+    st64 = LevelStepper(lev64, precision=abi.PREC_FP64, fuse=False, device=local)
     st64.step()
     tuned["fp64"] = autotune.tune(st64.plan, st64.dt, reps=3)
     st64.capture()
@@ -340,8 +340,10 @@ def run_ours(args):
 
     # ---- error of one mixed step against the FP64 form (bit-identical to the oracle)
     err = {}
-    sa = LevelStepper(wl.flame(n=args.n, box=args.box, seed=2 + rank), precision=abi.PREC_FP64, fuse=False)
-    sb = LevelStepper(wl.flame(n=args.n, box=args.box, seed=2 + rank), precision=abi.PREC_MIXED, fuse=True)
+    sa = LevelStepper(wl.flame(n=args.n, box=args.box, seed=2 + rank), precision=abi.PREC_FP64, fuse=False,
+                    device=local)
+    sb = LevelStepper(wl.flame(n=args.n, box=args.box, seed=2 + rank), precision=abi.PREC_MIXED, fuse=True,
+                    device=local)
     sa.step()
     sb.step()
     torch.cuda.synchronize()
@@ -369,7 +371,7 @@ def run_ours(args):
     if world == 1:
         host_in = torch.from_numpy(lev_e.state).pin_memory()
         host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
-        se = LevelStepper(lev_e, precision=abi.PREC_MIXED, fuse=True)
+        se = LevelStepper(lev_e, precision=abi.PREC_MIXED, fuse=True, device=local)
         h2d = d2h = se.row_bytes  # the valid rows each way; the step's ghost fill forms the rest
         for _ in range(2):
             se.upload(host_in)
@@ -388,7 +390,7 @@ def run_ours(args):
         e2e_serial = world * ncell * ke / (mse_serial / 1e3)
         se.close()
 
-        pipe = HostPipeline(lev_e, depth=3, precision=abi.PREC_MIXED, fuse=True)
+        pipe = HostPipeline(lev_e, depth=3, precision=abi.PREC_MIXED, fuse=True, device=local)
         assert (pipe.h2d_bytes, pipe.d2h_bytes) == (h2d, d2h)
         for i in range(3):
             pipe.submit(host_in, host_out[i % 2])
@@ -410,7 +412,7 @@ def run_ours(args):
     from particleclem_b200.serve import GpuExecutor, Scheduler, serve_sweep
 
     sp, _ = wl.serving_patches(nruns=16, per_run=args.serve_per_run, seed=5 + rank, eos=lev.eos)
-    sx = GpuExecutor(lev.eos, precision=abi.PREC_MIXED)
+    sx = GpuExecutor(lev.eos, precision=abi.PREC_MIXED, device=local)
     spids = [sx.add_patch(p) for p in sp]
     sx.start()
     Scheduler(sx, int(120e9)).run([sx.request(k, p, 0.0) for k, p in enumerate(spids[:4])])

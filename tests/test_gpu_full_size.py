@@ -3,8 +3,8 @@ depend on size: one step of a closed (periodic) level conserves total mass, mome
 energy and every species' mass to round-off, in the plain FP64 and the mixed form (each
 face flux is stored once and read by both of its cells, so the flux divergence telescopes
 over the domain; the reference's own check is Tests/test_masscons.py, rtol 1e-13). The
-256^3 periodic turbulence level (64 boxes of 64^3, one species) and the 128^3 flame level
-(64 boxes of 32^3, 9 species) closed in z."""
+256^3 periodic turbulence level (64 boxes of 64^3, one species; PPM and PLM) and the 128^3
+flame level (64 boxes of 32^3, 9 species) closed in z (PPM and hybrid WENO-Z5)."""
 import pytest
 import torch
 
@@ -28,11 +28,15 @@ def _totals(st):
     return v.sum(dim=(1, 2, 3)), v.abs().sum(dim=(1, 2, 3))
 
 
-@pytest.mark.parametrize("name", ["turbulence_256", "flame_128_closed"])
+CASES = [("turbulence_256", {}), ("flame_128_closed", {}), ("turbulence_256_plm", {"ppm_type": 0}),
+         ("flame_128_closed_weno_z5", {"use_hybrid_weno": True, "weno_scheme": 1})]
+
+
+@pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
 @pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
-def test_one_step_of_a_closed_level_conserves(name, prec):
-    lev = wl.turbulence(n=256, box=64, seed=4) if name == "turbulence_256" else _closed_flame()
-    st = LevelStepper(lev, precision=prec, fuse=prec == abi.PREC_MIXED)
+def test_one_step_of_a_closed_level_conserves(name, kw, prec):
+    lev = wl.turbulence(n=256, box=64, seed=4) if name.startswith("turbulence") else _closed_flame()
+    st = LevelStepper(lev, precision=prec, fuse=prec == abi.PREC_MIXED, **kw)
     before, scale = _totals(st)
     st.step()
     torch.cuda.synchronize()

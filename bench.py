@@ -59,50 +59,99 @@ def parse():
 
 
 # ---------------------------------------------------------------- clocks
-class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+def pci_bus_id(local):
+    """The PCI bus ID ("DDDDDDDD:BB:DD.0") of CUDA device ``local`` of this process, which
+    names the same physical GPU for NVML and nvidia-smi whatever CUDA_VISIBLE_DEVICES is."""
+    import torch
 
-    def __init__(self, gpu_index):
-        self.idx = gpu_index
-        self.proc = None
-        self.path = None
+    p = torch.cuda.get_device_properties(local)
+    return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+
+
+class ClockSampler:
+    """Samples the SM clock, power and clock-event reasons of the process's GPU (found by
+    its PCI bus ID) every ``period_s`` while the timed region runs: NVML from a thread
+    (read-only queries), or nvidia-smi at 100 ms where NVML is unavailable."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, local, period_s=0.01):
+        self.bus = pci_bus_id(local)
+        self.period = period_s
+        self.rows = []  # (sm_mhz, sm_max_mhz, power_w, reasons)
+        self.proc = self.path = self.thread = None
+        self.stop = False
+
+    def _nvml_loop(self, nv, h):
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1e3
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                rs = [n for n, c in self.REASONS if bits & getattr(nv, c)]
+                self.rows.append((float(sm), float(mx), pw, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={SMI_FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-        time.sleep(0.3)
+            import threading
+
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByPciBusId(self.bus)
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.bus}", f"--query-gpu={SMI_FIELDS}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            except OSError:
+                self.proc = None
+        time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
+        self.stop = True
+        if self.thread is not None:
+            self.thread.join(timeout=2)
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.path:
+            names = [n for n, _ in self.REASONS]
+            try:
+                for ln in open(self.path):
+                    f = [x.strip() for x in ln.split(",")]
+                    if len(f) >= 9:
+                        rs = [names[i] for i in range(4) if f[5 + i].lower().startswith("active")]
+                        self.rows.append((float(f[1]), float(f[2]), float(f[3]) if f[3] not in ("", "[N/A]") else 0.0,
+                                          rs))
+            finally:
+                os.unlink(self.path)
 
     def summary(self):
-        rows = []
-        try:
-            for ln in open(self.path):
-                f = [x.strip() for x in ln.split(",")]
-                if len(f) >= 9:
-                    rows.append(f)
-        finally:
-            os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        sm = sorted(float(r[1]) for r in rows)
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
-                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3] not in ("", "[N/A]"))}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0,
+                    "gpu": self.bus}
+        sm = sorted(r[0] for r in self.rows)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.rows[0][1],
+                "reasons": sorted({x for r in self.rows for x in r[3]}), "samples": len(self.rows),
+                "power_w_max": max(r[2] for r in self.rows), "gpu": self.bus,
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------- CPU baseline
@@ -199,6 +248,24 @@ def run_cpu_configs(args):
                           "runs": [round(r["value"]) for r in vals]}), flush=True)
         arm.pool.shutdown()
     return 0
+
+
+def rel_grouped(a, b, nspec):
+    """Per-component relative L1 and Linf of b against a (component-major CUDA tensors),
+    each component normalised by the sum / max of its physical group: mass (rho and the
+    species densities), momentum (three components), energy (rho E, rho e), temperature."""
+    import torch
+
+    nv = a.shape[0]
+    d = (a - b).abs().reshape(nv, -1)
+    r = a.abs().reshape(nv, -1)
+    s1, sinf = r.sum(1), r.max(1).values
+    g1, ginf = torch.ones_like(s1), torch.ones_like(s1)
+    for grp in ([0] + list(range(7, 7 + nspec)), [1, 2, 3], [4, 5], [6]):
+        grp = [c for c in grp if c < nv]
+        g1[grp] = s1[grp].max().clamp_min(1e-300)
+        ginf[grp] = sinf[grp].max().clamp_min(1e-300)
+    return (d.sum(1) / g1).cpu().numpy(), (d.max(1).values / ginf).cpu().numpy()
 
 
 def run_ours(args):
@@ -338,26 +405,39 @@ def run_ours(args):
     fp64_value = world * ncell * k64 / (ms64 / 1e3)
     st64.close()
 
-    # ---- error of one mixed step against the FP64 form (bit-identical to the oracle)
-    err = {}
+    # ---- error of one mixed step against the plain FP64 form. The FP64 form (reference
+    # operation order, per box) is the one the parity tests show bit-identical to the CPU
+    # oracle (hydro source and fluxes, 32^3 flame boxes of this level included), so these are
+    # errors against the oracle's arithmetic. Both outputs are compared: the updated state
+    # S_new (the bound 1e-6 applies to it) and the hydro source of the step.
     sa = LevelStepper(wl.flame(n=args.n, box=args.box, seed=2 + rank), precision=abi.PREC_FP64, fuse=False,
-                    device=local)
+                      device=local)
     sb = LevelStepper(wl.flame(n=args.n, box=args.box, seed=2 + rank), precision=abi.PREC_MIXED, fuse=True,
-                    device=local)
-    sa.step()
-    sb.step()
+                      device=local)
+    sa.fill()
+    sb.fill()
+    sa.plan.estdt(sa.cfl, sa.dt)
+    sb.dt.copy_(sa.dt)  # the same timestep on both sides: the difference is precision only
+    sa.plan.hydro(sa.dt)
+    sb.plan.hydro(sb.dt)
+    torch.cuda.synchronize()
+    src_l1, src_linf = rel_grouped(sa.hsrc.data, sb.hsrc.data, 9)
+    sa.plan.update(sa.dt)
+    sb.plan.update(sb.dt)
     torch.cuda.synchronize()
     g = 4
     A = sa.state.data[:, g:-g, g:-g, g:-g]
     B = sb.state.data[:, g:-g, g:-g, g:-g]
-    d = (A - B).abs().reshape(A.shape[0], -1)
-    ref = A.abs().reshape(A.shape[0], -1)
-    l1 = (d.sum(dim=1) / ref.sum(dim=1).clamp_min(1e-300)).cpu().numpy()
-    linf = (d.max(dim=1).values / ref.max(dim=1).values.clamp_min(1e-300)).cpu().numpy()
+    l1, linf = rel_grouped(A, B, 9)
     comp = ["rho", "mx", "my", "mz", "rhoE", "rhoe", "T"] + [f"rhoY{k}" for k in range(9)]
-    err = {"max_rel_l1": float(l1.max()), "max_rel_linf": float(linf.max()),
-           "per_component_rel_l1": {c: float(v) for c, v in zip(comp, l1)},
-           "dt_rel_diff": float(abs(sa.dt.item() - sb.dt.item()) / sa.dt.item())}
+    err = {"reference_side": "plain FP64 GPU form, per box, reference operation order: bit-identical to the CPU "
+                             "oracle in the parity tests",
+           "normalisation": "per component, by the sum (L1) / max (Linf) of its physical group (mass, momentum, "
+                            "energy, temperature)",
+           "s_new": {"max_rel_l1": float(l1.max()), "max_rel_linf": float(linf.max()),
+                     "per_component_rel_l1": {c: float(v) for c, v in zip(comp, l1)}},
+           "hydro_source": {"max_rel_l1": float(src_l1.max()), "max_rel_linf": float(src_linf.max())},
+           "bound": "max_rel_l1 of s_new <= 1e-6"}
     sa.close()
     sb.close()
 
@@ -447,7 +527,7 @@ def run_ours(args):
                             "form": "plain FP64, reference operation order, per-box (64 boxes), CUDA graph"
                                     + (", one level per GPU" if world > 1 else ""),
                             "speedup_of_mixed": value / fp64_value},
-            "error_vs_fp64": err,
+            "error_vs_fp64": err,  # errors against the oracle-equal FP64 form
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": mse / kp, "steps": kp,
                     "path": ("valid rows of a pinned host state -> H2D -> fill/estdt/hydro/update via C ABI -> "

@@ -17,7 +17,13 @@
  *
  * Every call is asynchronous on the given stream (NULL = legacy default stream) and
  * returns PCG_OK or a negative PCG_E* code; pcg_last_error() gives the message of the
- * calling thread's last failure. Nothing aborts the process. Calls are reentrant.
+ * calling thread's last failure. Nothing aborts the process. Calls may be made from
+ * several host threads at once (argument checks, plans and workspace are per call;
+ * the shared tables are locked), with one exception: the EOS tables live in device
+ * constant memory, one per species count, and pcg_set_eos_* replaces them with a
+ * synchronous copy that is NOT ordered with kernels already queued on other streams.
+ * Set the EOS once per run before advancing, or synchronise every stream that runs
+ * this library's kernels before setting it again.
  */
 #ifndef PCG_HYDRO_H
 #define PCG_HYDRO_H
@@ -70,8 +76,8 @@ typedef struct pcg_hydro_params {
   int32_t ppm_type;       /* 0 PLM, 1 PPM */
   int32_t plm_iorder;     /* 1, 2 or 4 */
   int32_t use_flattening;
-  int32_t use_hybrid_weno; /* must be 0 */
-  int32_t weno_scheme;
+  int32_t use_hybrid_weno; /* 1: hybrid WENO edge values in the PPM trace (ppm_type 1) */
+  int32_t weno_scheme;     /* with use_hybrid_weno: 0 WENO-JS5, 1 WENO-Z5, 2 WENO-Z7, 3 WENO-Z3 */
   int32_t domlo[3], domhi[3];
   int32_t bclo[3], bchi[3];
   int32_t nspec;          /* NUM_SPECIES: 1 (gamma law) or 9 (NASA-7 mixture) */
@@ -139,8 +145,10 @@ int pcg_hydro_box(const pcg_hydro_params* prm, const int32_t lo[3], const int32_
  * plugin's cudaMalloc can fail or fragment what is left, and some hosts forbid the
  * synchronisation cudaMalloc/cudaFree imply inside their step loop. This entry keeps
  * its tables and workspace in one 32 MiB static device array of the library and
- * calls no allocator. Limit: boxes up to 21^3 cells with 9 species or 27^3 with one
- * species in FP64 (25^3 / 31^3 mixed); larger boxes return PCG_EINVAL. The array's
+ * calls no allocator. Limit, without flux export: boxes up to 21^3 cells with 9 species
+ * or 27^3 with one species in FP64 (27^3 / 34^3 in the mixed form; a little more with
+ * flux export, whose fluxes live in the caller's arrays); larger boxes return
+ * PCG_EINVAL. The array's
  * address is looked up on the first call per device: make that call outside any
  * stream capture. All calls share the array, so calls that overlap on the GPU
  * (different streams or unordered host threads) race; calls on one stream do not. */

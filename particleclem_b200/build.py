@@ -1,9 +1,11 @@
 """Build the CUDA library in-tree: particleclem_b200/_lib/libpcg_hydro.so.
 
-Three translation units, all for sm_100a:
+Translation units, all for sm_100a (the kernel units once per species count, 1 and 9,
+compiled in parallel):
   pcg_kernels_strict.cu  FP64 kernels, --fmad=false (reference rounding, operation by operation)
-  pcg_kernels_fast.cu    FP64 with FMA contraction, and the mixed FP32/FP64 kernels
-                         (FP32 division and square root approximate)
+  pcg_kernels_fast.cu    FP64 with FMA contraction (and the FP64 step tail of the fast forms)
+  pcg_kernels_mixed.cu   the mixed form's FP32 stage kernels (FP32 division and square root
+                         approximate)
   pcg_host.cu            host runtime and the C ABI of include/pcg_hydro.h
 """
 from __future__ import annotations
@@ -23,13 +25,15 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", SRC, "-I", os.path.join(ROOT, "include")]
-UNITS = {
-    "pcg_kernels_strict.cu": ["--fmad=false"],
-    # FP32 division and square root as the hardware approximations (about 2 ulp): the
-    # mixed form's tolerance is 1e-6; FP64 arithmetic is not affected by these flags
-    "pcg_kernels_fast.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"],
-    "pcg_host.cu": [],
-}
+FAST = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+# (object tag, source, flags): each kernel unit is built once per species count
+UNITS = [(f"{name}_ns{ns}", f"pcg_kernels_{name}.cu", [*flags, f"-DPCG_TU_NS={ns}"])
+         for name, flags in (("strict", ["--fmad=false"]),
+                             # FP32 division and square root as the hardware approximations
+                             # (about 2 ulp): the mixed form's tolerance is 1e-6; FP64
+                             # arithmetic is not affected by these flags
+                             ("fast", FAST), ("mixed", FAST))
+         for ns in (1, 9)] + [("host", "pcg_host.cu", [])]
 
 
 def nvcc() -> str:
@@ -58,8 +62,8 @@ def build(force: bool = False, verbose: bool = False, out: str = LIB, extra=()) 
     tag = os.path.basename(out).replace(".so", "")
 
     def compile_unit(item):
-        src, extra_flags = item
-        obj = os.path.join(os.path.dirname(out), tag + "_" + src.replace(".cu", ".o"))
+        tag_u, src, extra_flags = item
+        obj = os.path.join(os.path.dirname(out), tag + "_" + tag_u + ".o")
         flags = list(extra_flags) + (list(extra) if src != "pcg_host.cu" else [])
         cmd = [cc, *COMMON, *ARCH, *flags, "-c", os.path.join(SRC, src), "-o", obj]
         if verbose:
@@ -69,8 +73,8 @@ def build(force: bool = False, verbose: bool = False, out: str = LIB, extra=()) 
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
         return obj
 
-    with ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
-        objs = list(ex.map(compile_unit, UNITS.items()))
+    with ThreadPoolExecutor(max_workers=min(len(UNITS), max(1, os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_unit, UNITS))
     tmp = out + ".tmp"
     cmd = [cc, "-shared", *ARCH, "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

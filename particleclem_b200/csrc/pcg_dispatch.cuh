@@ -1,12 +1,20 @@
-// pcg_dispatch.cuh -- per-translation-unit launch entry points. Included by
-// pcg_kernels_strict.cu (FP64, --fmad=false) and pcg_kernels_fast.cu (FMA allowed),
-// each with its own PCG_TU namespace and its own copy of the EOS constant bank.
+// pcg_dispatch.cuh -- per-translation-unit launch entry points. Each kernel translation
+// unit instantiates the stage kernels for ONE species count (PCG_TU_NS, 1 or 9) and one
+// arithmetic: PCG_TU_DOUBLE_ONLY (FP64 reference order, compiled --fmad=false),
+// PCG_TU_SINGLE_ONLY (the mixed form's FP32 stage kernels) or neither (FP64 with FMA
+// contraction, and the FP64 step tail of both fast forms). Each unit has its own
+// PCG_TU namespace and its own copy of the EOS constant bank; the host routes a call to
+// the unit of its (precision form, species count).
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include "pcg_kernels.cuh"
 #include "pcg_aux_kernels.cuh"
+
+#ifndef PCG_TU_NS
+#error "PCG_TU_NS (species count of this translation unit) must be defined"
+#endif
 
 namespace PCG_TU {
 
@@ -54,34 +62,38 @@ static cudaError_t launch_t(int stage, const pcg::StageArgs& a, int64_t nblocks,
   }
 }
 
-// ns: species count (1: gamma law, 9: NASA-7 mixture); single: FP32 compute type.
+// ns: species count (1: gamma law, 9: NASA-7 mixture); single: FP32 compute type. A
+// combination this unit does not hold is cudaErrorInvalidValue.
+constexpr int kNS = PCG_TU_NS;
+constexpr bool kMix = PCG_TU_NS > 1;
+
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
                          cudaStream_t s) {
-#ifdef PCG_TU_DOUBLE_ONLY
+  if (ns != kNS) return cudaErrorInvalidValue;
+#if defined(PCG_TU_DOUBLE_ONLY)
   if (single) return cudaErrorInvalidValue;
-  if (ns == 1) return launch_t<1, false, double>(stage, a, nblocks, variant, s);
-  if (ns == 9) return launch_t<9, true, double>(stage, a, nblocks, variant, s);
+  return launch_t<kNS, kMix, double>(stage, a, nblocks, variant, s);
+#elif defined(PCG_TU_SINGLE_ONLY)
+  if (!single) return cudaErrorInvalidValue;
+  return launch_t<kNS, kMix, float>(stage, a, nblocks, variant, s);
 #else
-  if (ns == 1)
-    return single ? launch_t<1, false, float>(stage, a, nblocks, variant, s)
-                  : launch_t<1, false, double>(stage, a, nblocks, variant, s);
-  if (ns == 9)
-    return single ? launch_t<9, true, float>(stage, a, nblocks, variant, s)
-                  : launch_t<9, true, double>(stage, a, nblocks, variant, s);
+  if (single) return cudaErrorInvalidValue;
+  return launch_t<kNS, kMix, double>(stage, a, nblocks, variant, s);
 #endif
-  return cudaErrorInvalidValue;
 }
 
+#if !defined(PCG_TU_SINGLE_ONLY)
 cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
-  if (ns == 1) return launch_advance_t<1, false>(a, nblocks, variant, s);
-  if (ns == 9) return launch_advance_t<9, true>(a, nblocks, variant, s);
-  return cudaErrorInvalidValue;
+  if (ns != kNS) return cudaErrorInvalidValue;
+  return launch_advance_t<kNS, kMix>(a, nblocks, variant, s);
 }
+#endif
 
+#if defined(PCG_TU_DOUBLE_ONLY)
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s) {
-  if (ns == 1) return launch_aux_t<1, false>(which, a, nblocks, s);
-  if (ns == 9) return launch_aux_t<9, true>(which, a, nblocks, s);
-  return cudaErrorInvalidValue;
+  if (ns != kNS) return cudaErrorInvalidValue;
+  return launch_aux_t<kNS, kMix>(which, a, nblocks, s);
 }
+#endif
 
 }  // namespace PCG_TU

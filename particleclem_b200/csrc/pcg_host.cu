@@ -22,19 +22,68 @@
 #include "../../include/pcg_hydro.h"
 #include "pcg_types.h"
 
+// The kernel translation units, one per (arithmetic, species count): see pcg_dispatch.cuh.
+#define PCG_DECL_TU(NAME)                                                                              \
+  namespace NAME {                                                                                     \
+  cudaError_t upload_eos(int slot, const pcg::EosConst& e);                                            \
+  cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks,  \
+                           int variant, cudaStream_t s);                                               \
+  }
+PCG_DECL_TU(pcg_strict1)
+PCG_DECL_TU(pcg_strict9)
+PCG_DECL_TU(pcg_fast1)
+PCG_DECL_TU(pcg_fast9)
+PCG_DECL_TU(pcg_mixed1)
+PCG_DECL_TU(pcg_mixed9)
+#undef PCG_DECL_TU
+#define PCG_DECL_ADV(NAME) \
+  namespace NAME { cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s); }
+PCG_DECL_ADV(pcg_strict1)
+PCG_DECL_ADV(pcg_strict9)
+PCG_DECL_ADV(pcg_fast1)
+PCG_DECL_ADV(pcg_fast9)
+#undef PCG_DECL_ADV
+namespace pcg_strict1 { cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s); }
+namespace pcg_strict9 { cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s); }
+
+// Routing by species count: pcg_strict = FP64 reference order (and the FP64 auxiliary
+// kernels), pcg_fast = FMA-contracted FP64 stages (single == false) or the mixed form's
+// FP32 stages (single == true), and the FP64 step tail of both fast forms.
 namespace pcg_strict {
-cudaError_t upload_eos(int slot, const pcg::EosConst& e);
-cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s);
+cudaError_t upload_eos(int slot, const pcg::EosConst& e) {
+  return slot == 0 ? pcg_strict1::upload_eos(slot, e) : pcg_strict9::upload_eos(slot, e);
+}
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
-                         cudaStream_t s);
-cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
+                         cudaStream_t s) {
+  return ns == 1 ? pcg_strict1::launch_stage(stage, ns, single, a, nblocks, variant, s)
+                 : pcg_strict9::launch_stage(stage, ns, single, a, nblocks, variant, s);
+}
+cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
+  return ns == 1 ? pcg_strict1::launch_advance(ns, a, nblocks, variant, s)
+                 : pcg_strict9::launch_advance(ns, a, nblocks, variant, s);
+}
+cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s) {
+  return ns == 1 ? pcg_strict1::launch_aux(which, ns, a, nblocks, s) : pcg_strict9::launch_aux(which, ns, a, nblocks, s);
+}
 }  // namespace pcg_strict
 namespace pcg_fast {
-cudaError_t upload_eos(int slot, const pcg::EosConst& e);
-cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s);
+cudaError_t upload_eos(int slot, const pcg::EosConst& e) {
+  cudaError_t r = slot == 0 ? pcg_fast1::upload_eos(slot, e) : pcg_fast9::upload_eos(slot, e);
+  if (r != cudaSuccess) return r;
+  return slot == 0 ? pcg_mixed1::upload_eos(slot, e) : pcg_mixed9::upload_eos(slot, e);
+}
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
-                         cudaStream_t s);
-cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s);
+                         cudaStream_t s) {
+  if (single)
+    return ns == 1 ? pcg_mixed1::launch_stage(stage, ns, single, a, nblocks, variant, s)
+                   : pcg_mixed9::launch_stage(stage, ns, single, a, nblocks, variant, s);
+  return ns == 1 ? pcg_fast1::launch_stage(stage, ns, single, a, nblocks, variant, s)
+                 : pcg_fast9::launch_stage(stage, ns, single, a, nblocks, variant, s);
+}
+cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
+  return ns == 1 ? pcg_fast1::launch_advance(ns, a, nblocks, variant, s)
+                 : pcg_fast9::launch_advance(ns, a, nblocks, variant, s);
+}
 }  // namespace pcg_fast
 
 namespace {
@@ -215,6 +264,8 @@ int check_params(const pcg_hydro_params* p) {
   if (p->ppm_type != 0 && p->ppm_type != 1) return fail(PCG_EINVAL, "PeleC::ppm_type must be 0 (PLM) or 1 (PPM)");
   if (p->use_hybrid_weno && p->ppm_type != 1)
     return fail(PCG_EINVAL, "PeleC::ppm_type must be 1 (PPM) to use WENO method");
+  if (p->use_hybrid_weno && (p->weno_scheme < 0 || p->weno_scheme > 3))
+    return fail(PCG_EINVAL, "weno_scheme %d: 0 WENO-JS5, 1 WENO-Z5, 2 WENO-Z7 or 3 WENO-Z3", p->weno_scheme);
   if (p->ppm_type == 0 && p->plm_iorder != 1 && p->plm_iorder != 2 && p->plm_iorder != 4)
     return fail(PCG_EINVAL, "plm_iorder must be 1, 2 or 4");
   if (p->precision_mode < PCG_PREC_FP64 || p->precision_mode > PCG_PREC_MIXED)
@@ -1199,8 +1250,9 @@ int pcg_plan_destroy(pcg_plan* P) {
 // array of the library instead.
 //
 // * kNoAllocScratchBytes (32 MiB) is the whole budget: enough for a box of up to 21^3
-//   cells with 9 species or 27^3 with one species in FP64 (25^3 / 31^3 in the mixed
-//   form). Larger boxes are rejected with PCG_EINVAL and a message giving both sizes.
+//   cells with 9 species or 27^3 with one species in FP64 (27^3 / 34^3 in the mixed
+//   form), without flux export. Larger boxes are rejected with PCG_EINVAL and a message
+//   giving both sizes.
 // * Every GPU that loads the library keeps the 32 MiB array until the process exits.
 // * The array's device address comes from cudaGetSymbolAddress, once per device, on
 //   the first call made with that device current (host code cannot use the symbol

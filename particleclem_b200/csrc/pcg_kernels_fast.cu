@@ -1,4 +1,6 @@
-// Fast kernels: FP64 with FMA contraction, and the mixed form (FP32 trace/Riemann/
-// transverse arithmetic, FP64 state, update, Newton and dt).
-#define PCG_TU pcg_fast
+// FP64 kernels with FMA contraction (PCG_PREC_FP64_FAST), and the FP64 step tail both
+// fast forms share. Built once per species count into pcg_fast1 / pcg_fast9.
+#define PCG_CAT2(a, b) a##b
+#define PCG_CAT(a, b) PCG_CAT2(a, b)
+#define PCG_TU PCG_CAT(pcg_fast, PCG_TU_NS)
 #include "pcg_dispatch.cuh"

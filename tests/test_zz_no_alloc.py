@@ -76,3 +76,25 @@ def test_noalloc_refuses_boxes_beyond_its_scratch():
     assert rc == -1
     msg = native.load().pcg_last_error().decode()
     assert "scratch" in msg and "pcg_hydro_box" in msg
+
+
+@pytest.mark.parametrize("prec,edge", [(abi.PREC_FP64, 21), (abi.PREC_MIXED, 27)])
+def test_noalloc_accepts_the_largest_stated_box_and_refuses_the_next(prec, edge):
+    """The stated limits with 9 species and no flux export: 21^3 in FP64 and 27^3 in the
+    mixed form run (and equal pcg_hydro_box bit for bit), one cell more per edge is refused."""
+    hydro.init(0)
+    hydro.set_eos(eos9())
+    nv = abi.nvar(9)
+    p = wl.flame_patch((edge, edge, edge), 9)
+    prm = abi.make_params(p.dx, 2e-8, 9, (-BIG,) * 3, (BIG,) * 3, (0, 0, 0), (0, 0, 0), precision_mode=prec)
+    uin = to_gpu(p.fab)
+    out = gpu_zeros(nv, p.lo, p.hi)
+    rc = _call_noalloc(prm, p.lo, p.hi, uin, out, None)
+    assert rc == 0, native.load().pcg_last_error().decode()
+    ref = gpu_zeros(nv, p.lo, p.hi)
+    hydro.hydro_box(prm, p.lo, p.hi, uin, ref)
+    np.testing.assert_array_equal(to_cpu(out), to_cpu(ref))
+    big = wl.flame_patch((edge + 1, edge + 1, edge + 1), 10)
+    uin2 = to_gpu(big.fab)
+    out2 = gpu_zeros(nv, big.lo, big.hi)
+    assert _call_noalloc(prm, big.lo, big.hi, uin2, out2, None) == -1

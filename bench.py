@@ -51,7 +51,9 @@ def parse():
     ap.add_argument("--box", type=int, default=32, help="box edge")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline work budget")
-    ap.add_argument("--serve-per-run", type=int, default=4, help="requests per ensemble run in the serving check")
+    ap.add_argument("--serve-requests", type=int, default=5000, help="step requests per serving load point")
+    ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0])
+    ap.add_argument("--serve-batch-cells", type=int, default=2_000_000, help="cells per serving batch at most")
     ap.add_argument("--cpu-configs", action="store_true",
                     help="only time the CPU baseline on the Sod box, the flame level and the turbulence level "
                          "(PPM and PLM), one JSON line each")
@@ -487,18 +489,14 @@ def run_ours(args):
         e2e_value = world * ncell * kp / (mse / 1e3)
         pipe.close()
 
-    # ---- serving: patch-advance latency under Poisson arrivals with continuous batching
-    # (16 ensemble runs submitting flame boxes of edges 16..64, HBM budget 120 GB)
-    from particleclem_b200.serve import GpuExecutor, Scheduler, serve_sweep
+    # ---- serving: patch-step latency under Poisson arrivals with continuous batching
+    # (16 ensemble runs x 32 flame patches of edges in {16..64}; every request one step of
+    # a resident, evolving patch; HBM budget 120 GB; two streams)
+    from particleclem_b200.serve import ensemble_serving
 
-    sp, _ = wl.serving_patches(nruns=16, per_run=args.serve_per_run, seed=5 + rank, eos=lev.eos)
-    sx = GpuExecutor(lev.eos, precision=abi.PREC_MIXED, device=local)
-    spids = [sx.add_patch(p) for p in sp]
-    sx.start()
-    Scheduler(sx, int(120e9)).run([sx.request(k, p, 0.0) for k, p in enumerate(spids[:4])])
-    sx.synchronize()
-    serving = serve_sweep(sx, spids, int(120e9), loads=(0.5, 0.9))
-    del sx
+    serving = ensemble_serving(lev.eos, nruns=16, per_run=32, seed=5 + rank, nreq=args.serve_requests,
+                               budget_bytes=int(120e9), loads=tuple(args.serve_loads),
+                               max_batch_cells=args.serve_batch_cells, error_sample=32, device=local)
 
     # ---- roofline: the dominant kernel (one fused region of the whole level) and the step
     from particleclem_b200 import roofline as rl
@@ -538,10 +536,15 @@ def run_ours(args):
                             "-> D2H, every step",
                     "serial": {"value": e2e_serial, "ms_per_step": mse_serial / ke,
                                "path": "same copies and step, one after another"}},
-            "serving": {"workload": f"16 runs x {args.serve_per_run} flame boxes, edges in {{16..64}}, ns9, mixed",
-                        "budget_gb": 120, "saturated_cell_updates_per_s": serving[0]["cell_updates_per_s"],
-                        "loads": [{k: r[k] for k in ("load", "p50_ms", "p99_ms", "cell_updates_per_s", "batches")}
-                                  for r in serving[1:]]},
+            "serving": {"workload": serving["workload"], "budget_gb": serving["budget_gb"],
+                        "max_batch_cells": serving["max_batch_cells"],
+                        "resident_state_gb": serving["resident_state_gb"],
+                        "saturated_cell_updates_per_s": serving["points"][0]["cell_updates_per_s"],
+                        "saturated_requests_per_s": serving["points"][0]["requests_per_s"],
+                        "loads": [{k: r[k] for k in ("load", "requests", "p50_ms", "p99_ms", "cell_updates_per_s",
+                                                     "batches", "peak_bytes")}
+                                  for r in serving["points"][1:]],
+                        "error_vs_fp64_one_step": serving["error_vs_fp64_one_step"]},
             "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 1, stages 6, fused tail 1, final dt 1
             "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},

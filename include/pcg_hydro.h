@@ -132,6 +132,26 @@ int pcg_umdrv(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi
               const pcg_array4* qaux, const pcg_array4* src_q, pcg_array4* flx,
               const pcg_array4* area, const pcg_array4* vol, pcg_stream_t stream);
 
+/* pc_srctoprim over [lo,hi] (Source/Hydro.H:14-68): the primitive-variable sources
+ * srcq (QVAR comps) from the conserved sources src (NVAR comps, PeleC's
+ * sources_for_hydro) and q, qaux. Replaces the launch at Source/Hydro.cpp:161-174; call
+ * it over grow(bx,4) to feed pcg_umdrv / pcg_umeth. Always FP64 (reference order). */
+int pcg_srctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+                  const pcg_array4* q, const pcg_array4* qaux, const pcg_array4* src,
+                  pcg_array4* srcq, pcg_stream_t stream);
+
+/* pc_umeth_3D on its own (Source/Godunov.cpp:59-476, declared Source/Godunov.H:1142-1162):
+ * from q, qaux and src_q on grow(bx,4) (src_q may be NULL: no sources), flx[d] receives
+ * the Godunov fluxes on the d-faces of bx as pc_umeth_3D leaves them (before the
+ * artificial viscosity, species normalisation and area weighting of pc_adjust_fluxes;
+ * component UTEMP is not written), qec[d] (NGDNV = 6 comps) the face states GDU, GDV, GDW,
+ * GDPRES, GDGAME (GDRHO is not written, as in the reference), and pdivu the p div u of
+ * Source/Godunov.H:1033-1060 on bx. area[3] and vol are the geometry FABs. */
+int pcg_umeth(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3],
+              const pcg_array4* q, const pcg_array4* qaux, const pcg_array4* src_q,
+              pcg_array4* flx, pcg_array4* qec, const pcg_array4* area, pcg_array4* pdivu,
+              const pcg_array4* vol, pcg_stream_t stream);
+
 /* One construct_hydro_source box iteration (Source/Hydro.cpp:70-249 for a regular
  * box, no sources): ctoprim on grow(bx,4), then pc_umdrv. uout is zeroed first;
  * flx may be NULL. Geometry is uniform Cartesian from prm->dx. */
@@ -164,6 +184,21 @@ int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t lo[3], cons
  * bc* are ignored). Uniform Cartesian geometry. */
 int pcg_hydro_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes,
                     pcg_stream_t stream);
+
+/* One full step of every box of a list of independent patches, each with its own
+ * timestep: the step PeleC's level advance takes around construct_hydro_source
+ * (Source/Advance.cpp:266-352) for a patch that is its own domain. Per box, in one set of
+ * launches over all boxes: with fill_ghosts != 0, the ghost cells of boxes[b].uin (4
+ * layers) from its own valid cells (periodic in a direction whose two boundary types are
+ * PCG_BC_INTERIOR, zero-gradient otherwise); the hydro stages with timestep dt[b]
+ * (dt: DEVICE array of nbox; NULL: boxes[b].dt); then S_new = S_old + dt hydro_source
+ * with computeTemp, written over boxes[b].uin (the hydro source itself is not stored;
+ * boxes[b].uout may be NULL); and dt_next[b] (DEVICE array of nbox) = cfl * the CFL
+ * minimum of the box's new state (Source/Timestep.H:51-88), its next timestep.
+ * Workspace as pcg_hydro_boxes. No counterpart in the reference (the serving loop of this
+ * library advances ensemble patches with it). */
+int pcg_step_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes, int32_t fill_ghosts,
+                   double cfl, const double* dt, double* dt_next, pcg_stream_t stream);
 
 /* Device bytes a pcg_hydro_boxes call over boxes [lo[3b], hi[3b]] (b < nbox) allocates
  * for its workspace and launch tables (stream-ordered, freed when the call's work

@@ -1437,6 +1437,39 @@ int orc_hydro_box(const orc_params* prm, const int32_t lo[3], const int32_t hi[3
   return rc;
 }
 
+/* Source/Hydro.cpp:161-174: pc_srctoprim (Source/Hydro.H:14-68) over a box. */
+int orc_srctoprim(const int32_t lo[3], const int32_t hi[3], const orc_array4* q, const orc_array4* qaux,
+                  const orc_array4* src, orc_array4* srcq) {
+  fab_t qf = fab_view(q), af = fab_view(qaux), sf = fab_view(src), of = fab_view(srcq);
+  box_t b = mkbox(lo, hi);
+  FOR_BOX(b, i, j, k) srctoprim_cell(i, j, k, &qf, &af, &sf, &of);
+  return 0;
+}
+
+/* pc_umeth_3D (Source/Godunov.cpp:59-476, declared Source/Godunov.H:1142-1162) on its own:
+ * flx[d] receives the final Godunov fluxes on the d-faces of the box (before the
+ * artificial viscosity, species normalisation and area weighting of pc_adjust_fluxes),
+ * qec[d] the face states GDU, GDV, GDW, GDPRES, GDGAME (GDRHO is not written, as in the
+ * reference), pdivu the cell-centred p div u. srcq may be NULL (no sources). */
+int orc_umeth(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], const orc_array4* q,
+              const orc_array4* qaux, const orc_array4* srcq, orc_array4* flx, orc_array4* qec,
+              const orc_array4* area, orc_array4* pdivu, const orc_array4* vol) {
+  if (prm->nspec != g_ns) return -3;
+  const box_t bx = mkbox(lo, hi);
+  fab_t qf = fab_view(q), af = fab_view(qaux), pf = fab_view(pdivu), vf = fab_view(vol);
+  fab_t sf, *sfp = NULL;
+  if (srcq) { sf = fab_view(srcq); sfp = &sf; }
+  fab_t ff[3], gf[3], aa[3];
+  for (int d = 0; d < 3; ++d) {
+    ff[d] = fab_view(&flx[d]);
+    gf[d] = fab_view(&qec[d]);
+    aa[d] = fab_view(&area[d]);
+  }
+  return umeth_3d(bx, prm->bclo, prm->bchi, prm->domlo, prm->domhi, &qf, &af, sfp, ff, gf, aa, &pf, &vf, prm->dx,
+                  prm->dt, prm->ppm_type, prm->plm_iorder, prm->use_flattening, prm->use_hybrid_weno,
+                  prm->weno_scheme);
+}
+
 /* ---------------------------------------------------------------- timestep */
 /* Source/Timestep.H:51-88 (pc_estdt_hydro), regular cells. */
 double orc_estdt(const int32_t lo[3], const int32_t hi[3], const orc_array4* u, const double dx[3]) {

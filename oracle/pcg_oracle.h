@@ -73,6 +73,13 @@ int orc_umdrv(const orc_params* prm, const int32_t lo[3], const int32_t hi[3],
 
 /* One construct_hydro_source box iteration: ctoprim on grow(bx,4), zero sources,
  * pc_umdrv. hydro_source (uout) is zeroed first, as Hydro.cpp:47 does. */
+/* pc_srctoprim over [lo, hi] (Source/Hydro.H:14-68). */
+int orc_srctoprim(const int32_t lo[3], const int32_t hi[3], const orc_array4* q, const orc_array4* qaux,
+                  const orc_array4* src, orc_array4* srcq);
+/* pc_umeth_3D alone (Source/Godunov.H:1142-1162): final fluxes, qec, pdivu. */
+int orc_umeth(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], const orc_array4* q,
+              const orc_array4* qaux, const orc_array4* srcq, orc_array4* flx, orc_array4* qec,
+              const orc_array4* area, orc_array4* pdivu, const orc_array4* vol);
 int orc_hydro_box(const orc_params* prm, const int32_t lo[3], const int32_t hi[3],
                   const orc_array4* uin, orc_array4* uout, orc_array4* flx,
                   const orc_array4* area, const orc_array4* vol);

@@ -71,6 +71,8 @@ class CpuHydro:
         self._f("ctoprim", [I3, I3, A4, A4, A4], C.c_int)
         self._f("umdrv", [P(abi.HydroParams), I3, I3, A4, A4, A4, A4, A4, A4, A4, A4], C.c_int)
         self._f("hydro_box", [P(abi.HydroParams), I3, I3, A4, A4, A4, A4, A4], C.c_int)
+        self._f("srctoprim", [I3, I3, A4, A4, A4, A4], C.c_int)
+        self._f("umeth", [P(abi.HydroParams), I3, I3, A4, A4, A4, A4, A4, A4, A4, A4], C.c_int)
         self._f("estdt", [I3, I3, A4, P(C.c_double)], C.c_double)
         self._f("update_state", [I3, I3, A4, A4, C.c_double, A4], C.c_int)
         self.eos = None
@@ -120,6 +122,38 @@ class CpuHydro:
         if rc != 0:
             raise RuntimeError(f"{self.prefix}_ctoprim returned {rc}")
         return q, qa
+
+    def srctoprim(self, lo, hi, q: abi.Fab, qa: abi.Fab, src: abi.Fab):
+        """pc_srctoprim over [lo, hi]: the primitive sources srcQ (QVAR components)."""
+        shp = tuple(hi[e] - lo[e] + 1 for e in (2, 1, 0))
+        sq = abi.Fab(np.zeros((abi.qvar(self.eos.nspec),) + shp), tuple(lo))
+        rc = self._srctoprim(abi.ivec(lo), abi.ivec(hi), C.byref(abi.array4(q)), C.byref(abi.array4(qa)),
+                             C.byref(abi.array4(src)), C.byref(abi.array4(sq)))
+        if rc != 0:
+            raise RuntimeError(f"{self.prefix}_srctoprim returned {rc}")
+        return sq
+
+    def umeth(self, prm, lo, hi, q: abi.Fab, qa: abi.Fab, srcq=None, area=None, vol=None):
+        """pc_umeth_3D alone: returns (flx[3], qec[3], pdivu) on the faces / cells of the box;
+        qec component GDRHO is left zero (the reference does not write it)."""
+        nv = abi.nvar(self.eos.nspec)
+        flx, qec = [], []
+        for d in range(3):
+            nlo, nhi = abi.nodes(lo, hi, d)
+            shp = tuple(nhi[e] - nlo[e] + 1 for e in (2, 1, 0))
+            flx.append(abi.Fab(np.zeros((nv,) + shp), nlo))
+            qec.append(abi.Fab(np.zeros((abi.NGDNV,) + shp), nlo))
+        shp = tuple(hi[e] - lo[e] + 1 for e in (2, 1, 0))
+        pdivu = abi.Fab(np.zeros((1,) + shp), tuple(lo))
+        if area is None:
+            area, vol = uniform_geometry(lo, hi, tuple(prm.dx))
+        rc = self._umeth(C.byref(prm), abi.ivec(lo), abi.ivec(hi), C.byref(abi.array4(q)), C.byref(abi.array4(qa)),
+                         C.byref(abi.array4(srcq)) if srcq is not None else None, abi.array4_list(flx),
+                         abi.array4_list(qec), abi.array4_list(area), C.byref(abi.array4(pdivu)),
+                         C.byref(abi.array4(vol)))
+        if rc != 0:
+            raise RuntimeError(f"{self.prefix}_umeth returned {rc}")
+        return flx, qec, pdivu
 
     def estdt(self, lo, hi, u: abi.Fab, dx):
         dxa = (C.c_double * 3)(*dx)

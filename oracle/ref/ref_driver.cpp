@@ -113,6 +113,40 @@ int ref_umdrv(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], c
   return umdrv(prm, bx, view(uin), view(uout), view(q), view(qaux), sq, f, a, view(vol));
 }
 
+// The launch of Source/Hydro.cpp:161-174: the reference's pc_srctoprim over a box.
+int ref_srctoprim(const int32_t lo[3], const int32_t hi[3], const orc_array4* q, const orc_array4* qaux,
+                  const orc_array4* src, orc_array4* srcq) {
+  amrex::Array4<const amrex::Real> qa = view(q), aa = view(qaux), sa = view(src);
+  auto oa = view(srcq);
+  amrex::ParallelFor(mkbox(lo, hi), [=](int i, int j, int k) { pc_srctoprim(i, j, k, qa, aa, sa, oa); });
+  return 0;
+}
+
+// The reference's pc_umeth_3D (Source/Godunov.cpp:59-476) called directly.
+int ref_umeth(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], const orc_array4* q,
+              const orc_array4* qaux, const orc_array4* srcq, orc_array4* flx, orc_array4* qec,
+              const orc_array4* area, orc_array4* pdivu, const orc_array4* vol) {
+  if (prm->nspec != NUM_SPECIES) return -3;
+  if (prm->ppm_type != 0 && prm->ppm_type != 1) return -2;
+  const amrex::Box bx = mkbox(lo, hi);
+  amrex::FArrayBox zero_src;
+  amrex::Array4<const amrex::Real> sq;
+  if (srcq) {
+    sq = view(srcq);
+  } else {
+    zero_src.resize(grow(bx, 4), QVAR);
+    sq = zero_src.const_array();
+  }
+  const amrex::GpuArray<const amrex::Array4<amrex::Real>, 3> f{{view(&flx[0]), view(&flx[1]), view(&flx[2])}};
+  const amrex::GpuArray<const amrex::Array4<amrex::Real>, 3> g{{view(&qec[0]), view(&qec[1]), view(&qec[2])}};
+  const amrex::GpuArray<const amrex::Array4<const amrex::Real>, 3> a{{view(&area[0]), view(&area[1]), view(&area[2])}};
+  const amrex::GpuArray<amrex::Real, 3> dx{{prm->dx[0], prm->dx[1], prm->dx[2]}};
+  pc_umeth_3D(bx, prm->bclo, prm->bchi, prm->domlo, prm->domhi, view(q), view(qaux), sq, f, g, a, view(pdivu),
+              view(vol), dx, prm->dt, prm->ppm_type, prm->plm_iorder, prm->use_flattening != 0,
+              prm->use_hybrid_weno != 0, prm->weno_scheme);
+  return 0;
+}
+
 // Source/Hydro.cpp:70-249 for one regular box, no sources (sources_for_hydro == 0).
 int ref_hydro_box(const orc_params* prm, const int32_t lo[3], const int32_t hi[3], const orc_array4* uin,
                   orc_array4* uout, orc_array4* flx, const orc_array4* area, const orc_array4* vol) {

@@ -191,6 +191,7 @@ struct Array4 {
     return i >= begin.x && i < end.x && j >= begin.y && j < end.y && k >= begin.z && k < end.z;
   }
   int nComp() const { return ncomp; }
+  T* dataPtr() const { return p; }
   explicit operator bool() const { return p != nullptr; }
 };
 

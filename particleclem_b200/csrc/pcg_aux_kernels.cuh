@@ -7,7 +7,7 @@
 
 namespace PCG_TU {
 
-enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL };
+enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES };
 
 __device__ __forceinline__ bool aux_item(const pcg::AuxArgs& a, const pcg::AuxBox*& bx, int& i, int& j, int& k) {
   const int64_t blk = blockIdx.x;
@@ -174,37 +174,70 @@ __device__ __forceinline__ int ghost_src(int c, int lo, int hi, bool periodic) {
   if (c > hi) return periodic ? c - n : hi;
   return c;
 }
-__global__ void __launch_bounds__(128) k_fill(pcg::AuxArgs a) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int ng = a.ng;
-  const int n0 = a.dhi[0] - a.dlo[0] + 1, n1 = a.dhi[1] - a.dlo[1] + 1, n2 = a.dhi[2] - a.dlo[2] + 1;
+// Ghost cell number t of the domain [dlo, dhi] grown by ng (t < the ghost-cell count) gets
+// its value from the valid cell the fill maps it to; false when t is past the last ghost.
+__device__ __forceinline__ bool fill_ghost(int64_t t, const int* dlo, const int* dhi, int ng, int periodic,
+                                          const pcg::View& state, int ncomp) {
+  const int n0 = dhi[0] - dlo[0] + 1, n1 = dhi[1] - dlo[1] + 1, n2 = dhi[2] - dlo[2] + 1;
   const int64_t e0 = n0 + 2 * ng, e1 = n1 + 2 * ng;
   const int64_t cz = e0 * e1 * 2 * ng, cy = e0 * 2 * ng * n2, cx = (int64_t)2 * ng * n1 * n2;
   int c[3];
   if (t < cz) {  // z ghost slabs: (i, j) over the grown extent, 2 ng layers
     const int g = (int)(t / (e0 * e1));
-    c[0] = (int)(t % e0) + a.dlo[0] - ng;
-    c[1] = (int)((t / e0) % e1) + a.dlo[1] - ng;
-    c[2] = (g < ng) ? a.dlo[2] - ng + g : a.dhi[2] + 1 + (g - ng);
+    c[0] = (int)(t % e0) + dlo[0] - ng;
+    c[1] = (int)((t / e0) % e1) + dlo[1] - ng;
+    c[2] = (g < ng) ? dlo[2] - ng + g : dhi[2] + 1 + (g - ng);
   } else if (t < cz + cy) {  // y ghost slabs of the valid k
     const int64_t u = t - cz;
     const int g = (int)((u / e0) % (2 * ng));
-    c[0] = (int)(u % e0) + a.dlo[0] - ng;
-    c[1] = (g < ng) ? a.dlo[1] - ng + g : a.dhi[1] + 1 + (g - ng);
-    c[2] = (int)(u / (e0 * 2 * ng)) + a.dlo[2];
+    c[0] = (int)(u % e0) + dlo[0] - ng;
+    c[1] = (g < ng) ? dlo[1] - ng + g : dhi[1] + 1 + (g - ng);
+    c[2] = (int)(u / (e0 * 2 * ng)) + dlo[2];
   } else if (t < cz + cy + cx) {  // x ghost slabs of the valid (j, k)
     const int64_t u = t - cz - cy;
     const int g = (int)(u % (2 * ng));
-    c[0] = (g < ng) ? a.dlo[0] - ng + g : a.dhi[0] + 1 + (g - ng);
-    c[1] = (int)((u / (2 * ng)) % n1) + a.dlo[1];
-    c[2] = (int)(u / ((int64_t)2 * ng * n1)) + a.dlo[2];
+    c[0] = (g < ng) ? dlo[0] - ng + g : dhi[0] + 1 + (g - ng);
+    c[1] = (int)((u / (2 * ng)) % n1) + dlo[1];
+    c[2] = (int)(u / ((int64_t)2 * ng * n1)) + dlo[2];
   } else {
-    return;
+    return false;
   }
   int src[3];
-  for (int d = 0; d < 3; ++d) src[d] = ghost_src(c[d], a.dlo[d], a.dhi[d], (a.periodic >> d) & 1);
-  const V4<double> s = v4<double>(a.state);
-  for (int comp = 0; comp < a.ncomp; ++comp) s(c[0], c[1], c[2], comp) = s(src[0], src[1], src[2], comp);
+  for (int d = 0; d < 3; ++d) src[d] = ghost_src(c[d], dlo[d], dhi[d], (periodic >> d) & 1);
+  const V4<double> s = v4<double>(state);
+  for (int comp = 0; comp < ncomp; ++comp) s(c[0], c[1], c[2], comp) = s(src[0], src[1], src[2], comp);
+  return true;
+}
+
+// The ghost cells of many independent boxes (each its own domain) in one launch: the
+// block finds its box by binary search over the boxes' first blocks.
+__global__ void __launch_bounds__(128) k_fill_boxes(pcg::AuxArgs a) {
+  const int64_t blk = blockIdx.x;
+  int lo = 0, hi = a.nfill - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.fills[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
+  }
+  const pcg::FillBox& f = a.fills[lo];
+  const int64_t t = (blk - f.blk0) * blockDim.x + threadIdx.x;
+  if (t >= f.count) return;
+  fill_ghost(t, f.dlo, f.dhi, a.ng, f.periodic, f.state, a.ncomp);
+}
+
+// The next timestep of every box of a batched step: block b reduces the CFL minima the
+// fused tail left for region b (the blocks of its advance segment), times cfl, into
+// dt_boxes[b].
+__global__ void __launch_bounds__(128) k_estdt_boxes(pcg::AuxArgs a) {
+  const pcg::Seg& sg = a.bsegs[blockIdx.x];
+  const int64_t nb = (sg.count + 127) / 128;
+  double v = DBL_MAX;
+  for (int64_t b = threadIdx.x; b < nb; b += blockDim.x) v = dmin(v, a.partial[sg.blk0 + b]);
+  v = block_min(v);
+  if (threadIdx.x == 0) a.dt_boxes[blockIdx.x] = v * a.cfl;
+}
+
+__global__ void __launch_bounds__(128) k_fill(pcg::AuxArgs a) {
+  fill_ghost((int64_t)blockIdx.x * blockDim.x + threadIdx.x, a.dlo, a.dhi, a.ng, a.periodic, a.state, a.ncomp);
 }
 
 template <int NS, bool MIX>
@@ -229,6 +262,8 @@ static cudaError_t launch_aux_t(int which, const pcg::AuxArgs& a, int64_t nblock
     case AUX_ESTDT_FINAL: k_estdt_final<<<1, block, 0, s>>>(a); break;
     case AUX_UPDATE: k_update<NS, MIX><<<grid, block, 0, s>>>(a); break;
     case AUX_FILL: k_fill<<<grid, block, 0, s>>>(a); break;
+    case AUX_FILL_BOXES: k_fill_boxes<<<grid, block, 0, s>>>(a); break;
+    case AUX_ESTDT_BOXES: k_estdt_boxes<<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -626,6 +626,7 @@ struct FaceState {
 template <class R>
 struct RiemannOut {
   R ustar, frho, fun, fut1, fut2, feden, feint, gun, gpres;
+  R gut1, gut2, regd;  // the Godunov state's tangential velocities and rho*e (qint)
 };
 
 // Source/Riemann.H:9-200 (riemann), omega = rad = 0, bc_test_val = 1. The EOS calls
@@ -729,6 +730,9 @@ __device__ __forceinline__ void riemann_reduced(const FaceState<NS, R>& L, const
   o.feint = qint_iu * regd;
   o.gun = qint_iu;
   o.gpres = qint_gdpres;
+  o.gut1 = qint_iv1;
+  o.gut2 = qint_iv2;
+  o.regd = regd;
 }
 
 template <int NS, bool MIX, class R>
@@ -837,15 +841,20 @@ __device__ __forceinline__ void riemann(const FaceState<NS, R>& L, const FaceSta
   o.feint = qint_iu * regd;
   o.gun = qint_iu;
   o.gpres = qint_gdpres;
+  o.gut1 = qint_iv1;
+  o.gut2 = qint_iv2;
+  o.regd = regd;
 }
 
 // Source/Godunov.H:303-449 (pc_cmpflx): boundary overrides at the domain faces
 // (:378-418), the Riemann solve, and the upwinded species fluxes (:15-25, :438-441).
 // The face states are in absolute velocity order (u, v, w); fl[] receives URHO, UMX,
 // UMY, UMZ, UEDEN, UEINT and the species fluxes in absolute order. DIR is the normal.
-template <int NS, bool MIX, bool EXACT, int DIR, class R>
+// With QX, qx[0..2] also receive the Godunov state's tangential velocities (t1, t2 in
+// absolute order) and rho*e, from which pc_umeth_3D's qint GDGAME is formed.
+template <int NS, bool MIX, bool EXACT, int DIR, class R, bool QX = false>
 __device__ __forceinline__ void cmpflx(const R* ql, const R* qr, int idx, int bclo, int bchi, int domlo, int domhi,
-                                       R cav, R p0, R* fl, R& gun, R& gpres) {
+                                       R cav, R p0, R* fl, R& gun, R& gpres, R* qx = nullptr) {
   constexpr int t1 = (DIR == 0) ? 1 : 0;
   constexpr int t2 = (DIR == 2) ? 1 : 2;
   FaceState<NS, R> L, Rs;
@@ -903,6 +912,11 @@ __device__ __forceinline__ void cmpflx(const R* ql, const R* qr, int idx, int bc
   }
   gun = o.gun;
   gpres = o.gpres;
+  if constexpr (QX) {
+    qx[0] = o.gut1;
+    qx[1] = o.gut2;
+    qx[2] = o.regd;
+  }
 }
 
 }  // namespace PCG_TU

@@ -50,10 +50,27 @@ static cudaError_t launch_v(int stage, const pcg::StageArgs& a, const dim3& grid
   return cudaGetLastError();
 }
 
+// pcg_umeth's final stage (raw fluxes and face states), its low-order boundary faces and
+// p div u; pcg_srctoprim. One launch shape each.
+template <int NS, bool MIX, class R>
+static cudaError_t launch_special(int stage, const pcg::StageArgs& a, const dim3& grid, const dim3& block,
+                                  cudaStream_t s) {
+  switch (stage) {
+    case K_FLUX2: k_flux2<NS, MIX, kExact, R, 0, true><<<grid, block, 0, s>>>(a); break;
+    case K_LOWBC: k_lowbc<NS, MIX, kExact, R, true><<<grid, block, 0, s>>>(a); break;
+    case K_CONSUP: k_pdivu<NS><<<grid, block, 0, s>>>(a); break;
+    case K_SRCQ: k_srctoprim<NS><<<grid, block, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 template <int NS, bool MIX, class R>
 static cudaError_t launch_t(int stage, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
   if (nblocks <= 0) return cudaSuccess;
   const dim3 grid((unsigned)nblocks), block(128);
+  if (stage == K_SRCQ || (a.umeth && (stage == K_FLUX2 || stage == K_LOWBC || stage == K_CONSUP)))
+    return launch_special<NS, MIX, R>(stage, a, grid, block, s);
   switch (variant) {
     case 0: return launch_v<NS, MIX, R, 0>(stage, a, grid, block, s);
     case 1: return launch_v<NS, MIX, R, 1>(stage, a, grid, block, s);

@@ -90,9 +90,9 @@ namespace {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
 // launches that are not stages of their own: the low-order inflow/user_bc faces, run as
-// part of stage K_FLUX2 right after it
-enum { K_LOWBC = K_NSTAGE, K_NKIND };
-enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL };
+// part of stage K_FLUX2 right after it, and pc_srctoprim (pcg_srctoprim)
+enum { K_LOWBC = K_NSTAGE, K_SRCQ, K_NKIND };
+enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES };
 constexpr int kThreads = 128;
 constexpr size_t kAlign = 256;
 
@@ -291,12 +291,15 @@ struct BoxIn {
   double dx[3];
   double dt;
   pcg::View uin, uout, q, qa, srcq, area[3], vol, flx[3];
+  pcg::View qec[3], pdivu;  // pcg_umeth: the caller's face states and p div u
   bool internal_q;  // ctoprim into the workspace
   bool zero_uout;
+  bool umeth = false;  // pc_umeth_3D alone: raw fluxes, qec and pdivu (see pcg::Region::umeth)
 };
 
 struct Layout {
   int ns = 1;
+  int umeth = 0;  // the plan is a pcg_umeth call
   size_t esz = 8;  // compute-type size of the intermediates
   size_t ws_bytes = 0;
   std::vector<pcg::Region> regions;
@@ -406,8 +409,13 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
       add_seg(L, K_FLUX1, (int)r, d, nodes(grow_dir(g1, d, -1), d));
     }
     // mixed form without flux export: FP32 final fluxes (FP64 accumulation in k_consup)
-    R.ff_single = (single && !B.flx[0].p && !B.flx[1].p && !B.flx[2].p) ? 1 : 0;
+    R.ff_single = (single && !B.flx[0].p && !B.flx[1].p && !B.flx[2].p && !B.umeth) ? 1 : 0;
     const size_t fsz = R.ff_single ? 4 : 8;
+    R.umeth = B.umeth ? 1 : 0;
+    if (B.umeth) {
+      L.umeth = 1;
+      R.pdivu = B.pdivu;
+    }
     for (int d = 0; d < 3; ++d) {
       const IBox fb = nodes(B.bx, d);
       if (B.flx[d].p) {
@@ -415,7 +423,10 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
       } else {
         take(L, fb, nv, fsz, R.ff[d]);
       }
-      take(L, fb, 2, fsz, R.qec[d]);
+      if (B.umeth)
+        R.qec[d] = B.qec[d];
+      else
+        take(L, fb, 2, fsz, R.qec[d]);
       add_seg(L, K_FLUX2, (int)r, d, fb);
     }
     // Source/Godunov.cpp:440-468: faces of the box on an inflow or user_bc domain
@@ -461,7 +472,7 @@ void rebase_workspace(Layout& L, const std::vector<BoxIn>& boxes, char* base) {
       for (int o = 0; o < 3; ++o)
         if (o != d) rebase(R.fdo[d][o], base);
       if (!B.flx[d].p) rebase(R.ff[d], base);
-      rebase(R.qec[d], base);
+      if (!B.umeth) rebase(R.qec[d], base);
     }
   }
 }
@@ -511,6 +522,7 @@ int launch_kind(const Layout& L, const Tables& T, const pcg_hydro_params* p, int
   a.use_flattening = p->use_flattening;
   a.use_hybrid_weno = p->use_hybrid_weno;
   a.weno_scheme = p->weno_scheme;
+  a.umeth = L.umeth;
   a.difmag = p->difmag;
   a.dt_dev = dt_dev;
   const int var = kind < K_NSTAGE ? variant_of(p->precision_mode, L.ns, kind) : 0;
@@ -575,7 +587,7 @@ int box_from_params(const pcg_hydro_params* p, const int32_t* lo, const int32_t*
   return check_box_common(B.bx, B.dx, B.dt, B.bclo, B.bchi);
 }
 
-int box_from_desc(const pcg_box& b, int nv, BoxIn& B) {
+int box_from_desc(const pcg_box& b, int nv, BoxIn& B, bool need_uout = true) {
   B = BoxIn{};
   B.bx = mkbox(b.lo, b.hi);
   for (int d = 0; d < 3; ++d) {
@@ -589,7 +601,7 @@ int box_from_desc(const pcg_box& b, int nv, BoxIn& B) {
   int rc = check_box_common(B.bx, B.dx, B.dt, B.bclo, B.bchi);
   if (rc) return rc;
   if ((rc = check_array("box uin", &b.uin, grow(B.bx, 4), nv))) return rc;
-  if ((rc = check_array("box uout", &b.uout, B.bx, nv))) return rc;
+  if ((need_uout || b.uout.p) && (rc = check_array("box uout", &b.uout, B.bx, nv))) return rc;
   B.uin = view_of(&b.uin);
   B.uout = view_of(&b.uout);
   for (int d = 0; d < 3; ++d) {
@@ -832,6 +844,80 @@ int pcg_umdrv(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi
   return run_once(prm, boxes, K_PREP, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
 }
 
+int pcg_umeth(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* q,
+              const pcg_array4* qaux, const pcg_array4* src_q, pcg_array4* flx, pcg_array4* qec,
+              const pcg_array4* area, pcg_array4* pdivu, const pcg_array4* vol, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  std::vector<BoxIn> boxes(1);
+  BoxIn& B = boxes[0];
+  if ((rc = box_from_params(prm, lo, hi, B))) return rc;
+  const int nv = pcg::nvar(prm->nspec), nq = pcg::qvar(prm->nspec);
+  const IBox g4 = grow(B.bx, 4);
+  if ((rc = check_array("q", q, g4, nq))) return rc;
+  if ((rc = check_array("qaux", qaux, g4, pcg::NQAUX))) return rc;
+  if (src_q && src_q->p && (rc = check_array("src_q", src_q, g4, nq))) return rc;
+  if (!flx || !qec || !area || !pdivu || !vol) return fail(PCG_EINVAL, "flx, qec, area, pdivu and vol are required");
+  for (int d = 0; d < 3; ++d) {
+    if ((rc = check_array("flx", &flx[d], nodes(B.bx, d), nv))) return rc;
+    if ((rc = check_array("qec", &qec[d], nodes(B.bx, d), pcg::NGDNV))) return rc;
+    if ((rc = check_array("area", &area[d], nodes(B.bx, d), 1))) return rc;
+  }
+  if ((rc = check_array("pdivu", pdivu, B.bx, 1))) return rc;
+  if ((rc = check_array("vol", vol, B.bx, 1))) return rc;
+  B.q = view_of(q);
+  B.qa = view_of(qaux);
+  B.srcq = view_of(src_q);
+  B.vol = view_of(vol);
+  B.pdivu = view_of(pdivu);
+  for (int d = 0; d < 3; ++d) {
+    B.area[d] = view_of(&area[d]);
+    B.flx[d] = view_of(&flx[d]);
+    B.qec[d] = view_of(&qec[d]);
+  }
+  B.internal_q = false;
+  B.zero_uout = false;
+  B.umeth = true;
+  return run_once(prm, boxes, K_PREP, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pcg_srctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* q,
+                  const pcg_array4* qaux, const pcg_array4* src, pcg_array4* srcq, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  const IBox bx = mkbox(lo, hi);
+  if (!bx.ok()) return fail(PCG_EINVAL, "empty box");
+  const int nv = pcg::nvar(prm->nspec), nq = pcg::qvar(prm->nspec);
+  if ((rc = check_array("q", q, bx, nq)) || (rc = check_array("qaux", qaux, bx, pcg::NQAUX)) ||
+      (rc = check_array("src", src, bx, nv)) || (rc = check_array("srcq", srcq, bx, nq)))
+    return rc;
+  // a one-region table with only the srctoprim launch, on the caller's arrays
+  Layout L;
+  L.ns = prm->nspec;
+  pcg::Region R{};
+  R.q = view_of(q);
+  R.qa = view_of(qaux);
+  R.src = view_of(src);
+  R.srcq = view_of(srcq);
+  L.regions.push_back(R);
+  add_seg(L, K_SRCQ, 0, 0, bx);
+  Tables T;
+  pack_tables(L, T);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  CUDA_TRY(ws_alloc(&T.dev, T.bytes, s));
+  cudaError_t e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    bind_tables(T);
+    pcg_hydro_params p = *prm;
+    p.precision_mode = PCG_PREC_FP64;  // FP64 in every form, reference operation order
+    rc = launch_kind(L, T, &p, K_SRCQ, nullptr, s);
+  } else {
+    rc = fail(PCG_ECUDA, "table upload: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(T.dev, s);
+  return rc;
+}
+
 int pcg_hydro_box(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* uin,
                   pcg_array4* uout, pcg_array4* flx, pcg_stream_t stream) {
   int rc = check_params(prm);
@@ -866,6 +952,102 @@ int pcg_hydro_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* bo
   for (int b = 0; b < nbox; ++b)
     if ((rc = box_from_desc(boxes[b], pcg::nvar(prm->nspec), bs[b]))) return rc;
   return run_once(prm, bs, K_CTOPRIM, K_CONSUP, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pcg_step_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* boxes, int32_t fill_ghosts,
+                   double cfl, const double* dt, double* dt_next, pcg_stream_t stream) {
+  int rc = check_params(prm);
+  if (rc) return rc;
+  if (nbox < 0 || (nbox > 0 && !boxes) || (nbox > 0 && !dt_next)) return fail(PCG_EINVAL, "bad arguments");
+  if (!(cfl > 0.0) || !std::isfinite(cfl)) return fail(PCG_EINVAL, "cfl must be positive");
+  if (nbox == 0) return PCG_OK;
+  if ((rc = ensure_eos(prm->nspec))) return rc;
+  const int nv = pcg::nvar(prm->nspec);
+  std::vector<BoxIn> bs(nbox);
+  for (int b = 0; b < nbox; ++b)
+    if ((rc = box_from_desc(boxes[b], nv, bs[b], false))) return rc;
+  Layout L;
+  build_layout(L, bs, prm);
+  for (int b = 0; b < nbox; ++b) L.regions[b].dt_ptr = dt ? dt + b : nullptr;
+  // ghost fill table: each box is its own domain (periodic where both its boundary types
+  // are interior, zero-gradient elsewhere)
+  std::vector<pcg::FillBox> fills;
+  int64_t fill_blocks = 0;
+  if (fill_ghosts) {
+    for (int b = 0; b < nbox; ++b) {
+      pcg::FillBox f{};
+      f.state = bs[b].uin;
+      int64_t inner = 1, outer = 1;
+      for (int d = 0; d < 3; ++d) {
+        f.dlo[d] = bs[b].bx.lo[d];
+        f.dhi[d] = bs[b].bx.hi[d];
+        if (bs[b].bclo[d] == PCG_BC_INTERIOR && bs[b].bchi[d] == PCG_BC_INTERIOR) f.periodic |= 1 << d;
+        inner *= bs[b].bx.n(d);
+        outer *= bs[b].bx.n(d) + 8;
+      }
+      f.count = outer - inner;
+      f.blk0 = fill_blocks;
+      fill_blocks += (f.count + kThreads - 1) / kThreads;
+      fills.push_back(f);
+    }
+  }
+  // one stream-ordered allocation: [workspace | tables | fill table | block minima]
+  Tables T;
+  pack_tables(L, T);
+  const size_t off_t = (L.ws_bytes + kAlign - 1) / kAlign * kAlign;
+  const size_t off_f = off_t + (T.bytes + kAlign - 1) / kAlign * kAlign;
+  const size_t off_p = off_f + (fills.size() * sizeof(pcg::FillBox) + kAlign - 1) / kAlign * kAlign;
+  const size_t total = off_p + size_t(std::max<int64_t>(L.nblocks[K_CONSUP], 1)) * sizeof(double);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  void* mem = nullptr;
+  CUDA_TRY(ws_alloc(&mem, total, s));
+  char* base = static_cast<char*>(mem);
+  rebase_workspace(L, bs, base);
+  Tables T2;
+  pack_tables(L, T2);  // the regions now hold the workspace addresses
+  T2.dev = base + off_t;
+  std::vector<char> host(off_p - off_t, 0);
+  std::memcpy(host.data(), T2.host.data(), T2.bytes);
+  if (!fills.empty()) std::memcpy(host.data() + (off_f - off_t), fills.data(), fills.size() * sizeof(pcg::FillBox));
+  cudaError_t e = cudaMemcpyAsync(base + off_t, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(mem, s);
+    return fail(PCG_ECUDA, "table upload: %s", cudaGetErrorString(e));
+  }
+  bind_tables(T2);
+  double* partial = reinterpret_cast<double*>(base + off_p);
+  const bool strict = prm->precision_mode == PCG_PREC_FP64;
+  if (fill_ghosts) {
+    pcg::AuxArgs f{};
+    f.fills = reinterpret_cast<const pcg::FillBox*>(base + off_f);
+    f.nfill = nbox;
+    f.ng = 4;
+    f.ncomp = nv;
+    e = pcg_strict::launch_aux(AUX_FILL_BOXES, prm->nspec, f, fill_blocks, s);
+    if (e != cudaSuccess) rc = fail(PCG_ECUDA, "ghost fill: %s", cudaGetErrorString(e));
+  }
+  if (!rc) rc = launch_stages(L, T2, prm, K_CTOPRIM, K_FLUX2, nullptr, s);
+  if (!rc) {
+    pcg::StageArgs a{};
+    a.regions = T2.regions;
+    a.segs = T2.segs[K_CONSUP];
+    a.nseg = (int32_t)L.segs[K_CONSUP].size();
+    a.partial = partial;
+    const int v = variant_of(prm->precision_mode, prm->nspec, K_CONSUP);
+    e = strict ? pcg_strict::launch_advance(prm->nspec, a, L.nblocks[K_CONSUP], v, s)
+               : pcg_fast::launch_advance(prm->nspec, a, L.nblocks[K_CONSUP], v, s);
+    if (e == cudaSuccess) {
+      pcg::AuxArgs r{};
+      r.bsegs = T2.segs[K_CONSUP];
+      r.partial = partial;
+      r.cfl = cfl;
+      r.dt_boxes = dt_next;
+      e = pcg_strict::launch_aux(AUX_ESTDT_BOXES, prm->nspec, r, nbox, s);
+    }
+    if (e != cudaSuccess) rc = fail(PCG_ECUDA, "step tail: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(mem, s);
+  return rc;
 }
 
 int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t* lo, const int32_t* hi,

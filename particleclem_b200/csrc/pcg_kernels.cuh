@@ -26,7 +26,9 @@
 namespace PCG_TU {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
-enum { K_LOWBC = K_NSTAGE };  // inflow/user_bc boundary faces, launched within stage K_FLUX2
+// launches that are not stages of their own: the inflow/user_bc boundary faces (within
+// stage K_FLUX2) and pc_srctoprim (pcg_srctoprim)
+enum { K_LOWBC = K_NSTAGE, K_SRCQ };
 
 // Launch variants: each heavy stage is compiled with a few minimum-resident-blocks
 // requests (__launch_bounds__ register caps); the host picks one per (form, species
@@ -50,7 +52,7 @@ struct Item {
 // Timestep of a region and the constants the reference derives from it
 // (Source/Godunov.cpp:85-91, Source/PPM.cpp:37), with the same expressions.
 __device__ __forceinline__ double dt_of(const pcg::StageArgs& a, const pcg::Region& rg) {
-  return a.dt_dev ? *a.dt_dev : rg.dt;
+  return a.dt_dev ? *a.dt_dev : rg.dt_ptr ? *rg.dt_ptr : rg.dt;
 }
 
 __device__ __forceinline__ bool item_of(const pcg::StageArgs& a, Item& it) {
@@ -109,9 +111,12 @@ __device__ __forceinline__ int64_t dstride(const V4<T>& v, int d) {
 // conserved partial densities and the stored temperature (any constant of the region
 // would do; this one needs no neighbour, no division and no Newton solve, so every
 // stage computes the same value cheaply); zero for FP64.
+// A region without a conserved state (pcg_umeth, which takes only q and qaux) uses the
+// primitive pressure of the same cell.
 template <int NS, bool MIX, class R>
 __device__ __forceinline__ double p0_of(const pcg::Region& rg) {
   if constexpr (PDev<R>::on) {
+    if (!rg.uin.p) return v4<const double>(rg.q)(rg.lo[0], rg.lo[1], rg.lo[2], pcg::QPRES);
     const CellPtr<const double> u{&v4<const double>(rg.uin)(rg.lo[0], rg.lo[1], rg.lo[2], 0), rg.uin.ns};
     double w[NS];
 #pragma unroll
@@ -631,15 +636,15 @@ __device__ __forceinline__ void load_state(const CellPtr<R>& t, R* s) {
   for (int n = 0; n < pcg::nt_comps(NS); ++n) s[n] = t[n];
 }
 
-template <int NS, bool MIX, bool EXACT, int D, class R>
+template <int NS, bool MIX, bool EXACT, int D, class R, bool QX = false>
 __device__ __forceinline__ void face_flux(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr,
-                                          R* fl, R& gun, R& gpres) {
+                                          R* fl, R& gun, R& gpres, R* qx = nullptr) {
   const V4<const double> qav = v4<const double>(rg.qa);
   const CellPtr<const double> qa = at(qav, i, j, k);
   const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + (int64_t)pcg::QC * qa.ns]));
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
-  cmpflx<NS, MIX, EXACT, D, R>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav,
-                               R(p0_of<NS, MIX, R>(rg)), fl, gun, gpres);
+  cmpflx<NS, MIX, EXACT, D, R, QX>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav,
+                                   R(p0_of<NS, MIX, R>(rg)), fl, gun, gpres, qx);
 }
 
 template <int NS, class R>
@@ -1144,9 +1149,38 @@ __device__ __forceinline__ void flux2_state(const pcg::Region& rg, int i, int j,
 // of pc_adjust_fluxes (Source/Hydro.cpp:380-413): pc_artif_visc (Godunov.H:1067-1138),
 // pc_norm_spec_flx and pc_ext_flx (Hydro.H:835-865). ql and qr are the face's traced
 // states after their transverse corrections.
+// pc_umeth_3D's own outputs at one final face (Source/Godunov.cpp:392-438, and the
+// low-order boundary faces): the Godunov fluxes as pc_cmpflx leaves them, before
+// pc_adjust_fluxes (UTEMP is not a Riemann output and is left as the caller set it), and
+// the face state qint: GDU..GDW in absolute order, GDPRES and GDGAME = p / (rho e) + 1
+// (Source/Riemann.H:181); GDRHO is not written (nor is it by the reference).
 template <int NS, bool MIX, bool EXACT, int D, class R>
+__device__ __forceinline__ void umeth_face(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr,
+                                           double p0d) {
+  constexpr int t1 = (D == 0) ? 1 : 0;
+  constexpr int t2 = (D == 2) ? 1 : 2;
+  R flr[pcg::nvar(NS)], gun, gpres, qx[3];
+  face_flux<NS, MIX, EXACT, D, R, true>(rg, i, j, k, ql, qr, flr, gun, gpres, qx);
+  const CellPtr<double> ff = at(v4<double>(rg.ff[D]), i, j, k);
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n)
+    if (n != pcg::UTEMP) ff[n] = (PDev<R>::on && n == pcg::UMX + D) ? double(flr[n]) + p0d : double(flr[n]);
+  const CellPtr<double> qe = at(v4<double>(rg.qec[D]), i, j, k);
+  const double gp = PDev<R>::on ? double(gpres) + p0d : double(gpres);
+  qe[pcg::GDU + D] = double(gun);
+  qe[pcg::GDU + t1] = double(qx[0]);
+  qe[pcg::GDU + t2] = double(qx[1]);
+  qe[pcg::GDPRES] = gp;
+  qe[pcg::GDGAME] = EXACT ? double(gpres / qx[2] + R(1)) : gp / double(qx[2]) + 1.0;
+}
+
+template <int NS, bool MIX, bool EXACT, int D, class R, bool UMETH = false>
 __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k,
                                            const R* ql, const R* qr, double p0d) {
+  if constexpr (UMETH) {
+    umeth_face<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, p0d);
+    return;
+  }
   constexpr int O1 = (D == 0) ? 1 : 0;
   constexpr int O2 = (D == 2) ? 1 : 2;
   R flr[pcg::nvar(NS)], gun, gpres;
@@ -1218,7 +1252,7 @@ __device__ __forceinline__ void flux2_consts(const pcg::StageArgs& a, const pcg:
   p0d = p0_of<NS, MIX, R>(rg);
 }
 
-template <int NS, bool MIX, bool EXACT, class R>
+template <int NS, bool MIX, bool EXACT, class R, bool UMETH = false>
 __device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kx) {
   const pcg::Region& rg = a.regions[sg.region];
   const int64_t local = t * blockDim.x + threadIdx.x;
@@ -1249,10 +1283,10 @@ __device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg&
     for (int n = 0; n < ncorr<NS>(); ++n) K[n] = mine[n * 128 + 1];
   }
   flux2_state<NS, EXACT, 0, 1, R>(rg, i, j, k, K, hdt, p0, qr);
-  flux2_face<NS, MIX, EXACT, 0, R>(a, rg, i, j, k, ql, qr, p0d);
+  flux2_face<NS, MIX, EXACT, 0, R, UMETH>(a, rg, i, j, k, ql, qr, p0d);
 }
 
-template <int NS, bool MIX, bool EXACT, int D, class R>
+template <int NS, bool MIX, bool EXACT, int D, class R, bool UMETH = false>
 __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kcarry) {
   const pcg::Region& rg = a.regions[sg.region];
   int i, r, m0, m1;
@@ -1286,19 +1320,19 @@ __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::
     R* tmp = sl;
     sl = sr;
     sr = tmp;
-    flux2_face<NS, MIX, EXACT, D, R>(a, rg, i, j, k, ql, qr, p0d);
+    flux2_face<NS, MIX, EXACT, D, R, UMETH>(a, rg, i, j, k, ql, qr, p0d);
   }
 }
 
-template <int NS, bool MIX, bool EXACT, class R, int MINB>
+template <int NS, bool MIX, bool EXACT, class R, int MINB, bool UMETH = false>
 __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
   __shared__ R kcarry[2 * ncorr<NS>() * 128];
   int64_t t;
   const pcg::Seg& sg = seg_of(a, t);
   switch (sg.variant) {
-    case 0: flux2_x<NS, MIX, EXACT, R>(a, sg, t, kcarry); break;
-    case 1: flux2_march<NS, MIX, EXACT, 1, R>(a, sg, t, kcarry); break;
-    default: flux2_march<NS, MIX, EXACT, 2, R>(a, sg, t, kcarry); break;
+    case 0: flux2_x<NS, MIX, EXACT, R, UMETH>(a, sg, t, kcarry); break;
+    case 1: flux2_march<NS, MIX, EXACT, 1, R, UMETH>(a, sg, t, kcarry); break;
+    default: flux2_march<NS, MIX, EXACT, 2, R, UMETH>(a, sg, t, kcarry); break;
   }
 }
 
@@ -1308,7 +1342,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
 // cell's flattening, the cell's qaux sound speed) without transverse corrections; the
 // flux adjustments of pc_adjust_fluxes follow as for every face. Runs after K_FLUX2 and
 // overwrites its results on those faces.
-template <int NS, bool MIX, bool EXACT, int D, class R>
+template <int NS, bool MIX, bool EXACT, int D, class R, bool UMETH = false>
 __device__ __forceinline__ void lowbc_face(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
   const int di = (D == 0), dj = (D == 1), dk = (D == 2);
   const double dt = dt_of(a, rg);
@@ -1321,18 +1355,72 @@ __device__ __forceinline__ void lowbc_face(const pcg::StageArgs& a, const pcg::R
   // right state: the low-side state of the face's own cell
   plm_cell<NS, MIX, D, R>(rg, i, j, k, R(qav(i, j, k, pcg::QC)), prv(i, j, k, 0), a.plm_iorder, dt,
                           RegState<R>{qr}, RegState<R>{unused});
-  flux2_face<NS, MIX, EXACT, D, R>(a, rg, i, j, k, ql, qr, p0_of<NS, MIX, R>(rg));
+  flux2_face<NS, MIX, EXACT, D, R, UMETH>(a, rg, i, j, k, ql, qr, p0_of<NS, MIX, R>(rg));
 }
 
-template <int NS, bool MIX, bool EXACT, class R>
+template <int NS, bool MIX, bool EXACT, class R, bool UMETH = false>
 __global__ void __launch_bounds__(128) k_lowbc(pcg::StageArgs a) {
   Item it;
   if (!item_of(a, it)) return;
   switch (it.variant) {
-    case 0: lowbc_face<NS, MIX, EXACT, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
-    case 1: lowbc_face<NS, MIX, EXACT, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
-    default: lowbc_face<NS, MIX, EXACT, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+    case 0: lowbc_face<NS, MIX, EXACT, 0, R, UMETH>(a, *it.rg, it.i, it.j, it.k); break;
+    case 1: lowbc_face<NS, MIX, EXACT, 1, R, UMETH>(a, *it.rg, it.i, it.j, it.k); break;
+    default: lowbc_face<NS, MIX, EXACT, 2, R, UMETH>(a, *it.rg, it.i, it.j, it.k); break;
   }
+}
+
+// Source/Godunov.H:1033-1060 (pc_pdivu) from pc_umeth_3D's own face states (the caller's
+// NGDNV-component qec arrays of pcg_umeth), in the reference's expression order.
+template <int NS>
+__global__ void __launch_bounds__(128) k_pdivu(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  const pcg::Region& rg = *it.rg;
+  const int i = it.i, j = it.j, k = it.k;
+  const V4<const double> q0 = v4<const double>(rg.qec[0]), q1 = v4<const double>(rg.qec[1]),
+                         q2 = v4<const double>(rg.qec[2]);
+  const V4<const double> a0 = v4<const double>(rg.area[0]), a1 = v4<const double>(rg.area[1]),
+                         a2 = v4<const double>(rg.area[2]);
+  v4<double>(rg.pdivu)(i, j, k) =
+    0.5 *
+    ((q0(i + 1, j, k, pcg::GDPRES) + q0(i, j, k, pcg::GDPRES)) *
+       (q0(i + 1, j, k, pcg::GDU) * a0(i + 1, j, k) - q0(i, j, k, pcg::GDU) * a0(i, j, k)) +
+     (q1(i, j + 1, k, pcg::GDPRES) + q1(i, j, k, pcg::GDPRES)) *
+       (q1(i, j + 1, k, pcg::GDV) * a1(i, j + 1, k) - q1(i, j, k, pcg::GDV) * a1(i, j, k)) +
+     (q2(i, j, k + 1, pcg::GDPRES) + q2(i, j, k, pcg::GDPRES)) *
+       (q2(i, j, k + 1, pcg::GDW) * a2(i, j, k + 1) - q2(i, j, k, pcg::GDW) * a2(i, j, k))) /
+    v4<const double>(rg.vol)(i, j, k);
+}
+
+// Source/Hydro.H:14-68 (pc_srctoprim), launched over grow(bx,4) as at Source/Hydro.cpp:161-174:
+// the primitive-variable sources srcQ from the conserved sources src and q, qaux. Only the
+// components the reference writes are written (not QGAME, QTEMP).
+template <int NS>
+__global__ void __launch_bounds__(128) k_srctoprim(pcg::StageArgs a) {
+  Item it;
+  if (!item_of(a, it)) return;
+  const pcg::Region& rg = *it.rg;
+  const CellPtr<const double> q = at(v4<const double>(rg.q), it.i, it.j, it.k);
+  const CellPtr<const double> qa = at(v4<const double>(rg.qa), it.i, it.j, it.k);
+  const CellPtr<const double> src = at(v4<const double>(rg.src), it.i, it.j, it.k);
+  const CellPtr<double> sq = at(v4<double>(rg.srcq), it.i, it.j, it.k);
+  const double srcrho = src[pcg::URHO];
+  const double rhoinv = 1.0 / q[pcg::QRHO];
+  const double vx = q[pcg::QU];
+  const double vy = q[pcg::QV];
+  const double vz = q[pcg::QW];
+  const double umx = src[pcg::UMX];
+  const double umy = src[pcg::UMY];
+  const double umz = src[pcg::UMZ];
+  sq[pcg::QRHO] = srcrho;
+  sq[pcg::QU] = (umx - vx * srcrho) * rhoinv;
+  sq[pcg::QV] = (umy - vy * srcrho) * rhoinv;
+  sq[pcg::QW] = (umz - vz * srcrho) * rhoinv;
+  const double sreint = src[pcg::UEDEN] - vx * umx - vy * umy - vz * umz + srcrho * (vx * vx + vy * vy + vz * vz);
+  sq[pcg::QREINT] = sreint;
+  sq[pcg::QPRES] = qa[pcg::QDPDE] * (sreint - q[pcg::QREINT] * srcrho * rhoinv) * rhoinv + qa[pcg::QDPDR] * srcrho;
+#pragma unroll
+  for (int n = 0; n < NS; n++) sq[pcg::QFS + n] = (src[pcg::UFS + n] - q[pcg::QFS + n] * srcrho) * rhoinv;
 }
 
 // Source/Godunov.H:1033-1060 (pc_pdivu) and Source/Hydro.H:888-907 (pc_update), FP64

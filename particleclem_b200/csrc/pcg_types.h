@@ -16,6 +16,7 @@ namespace pcg {
 enum { URHO = 0, UMX = 1, UMY = 2, UMZ = 3, UEDEN = 4, UEINT = 5, UTEMP = 6, UFS = 7 };
 enum { QRHO = 0, QU = 1, QV = 2, QW = 3, QGAME = 4, QPRES = 5, QREINT = 6, QTEMP = 7, QFS = 8 };
 enum { QGAMC = 0, QC = 1, QCSML = 2, QDPDR = 3, QDPDE = 4, QRSPEC = 5, NQAUX = 6 };
+enum { GDRHO = 0, GDU = 1, GDV = 2, GDW = 3, GDPRES = 4, GDGAME = 5, NGDNV = 6 };
 // Source/PeleC.H:49-57
 enum { BC_INTERIOR = 0, BC_INFLOW, BC_OUTFLOW, BC_SYMMETRY, BC_SLIP_WALL, BC_NO_SLIP_WALL, BC_USER };
 
@@ -78,7 +79,8 @@ struct Region {
   int32_t lo[3], hi[3];
   int32_t domlo[3], domhi[3], bclo[3], bchi[3];
   double dx[3];
-  double dt;        // used unless StageArgs::dt_dev is set
+  double dt;        // used unless StageArgs::dt_dev or dt_ptr is set
+  const double* dt_ptr;  // device pointer to this region's own timestep (batched steps)
   double area_u[3]; // uniform face areas (used when area[d].p == nullptr)
   double vol_u;     // uniform volume (used when vol.p == nullptr)
   View uin;         // conserved state, double, >= 4 ghosts
@@ -102,6 +104,14 @@ struct Region {
   int32_t qf_in_prep; // 1: k_prep writes qf (no ctoprim stage), 0: k_ctoprim writes it
   int32_t ff_single;  // 1: ff/qec are FP32 with the pressure as deviation from p0
   int32_t qf_grow;    // qf covers grow(box, qf_grow): 3, or 4 for the 7-point WENO trace
+  // pc_umeth_3D on its own (pcg_umeth): the final stage writes the unadjusted Godunov
+  // fluxes into ff (FP64, caller's arrays, UTEMP untouched) and the face states into qec
+  // (the caller's NGDNV-component arrays, GDRHO untouched), and p div u goes to pdivu
+  // instead of the flux divergence
+  int32_t umeth;
+  int32_t pad2;
+  View pdivu;       // umeth: p div u on the box, double
+  View src;         // pcg_srctoprim: conserved sources, double, NVAR comps
 };
 
 // A run of thread blocks of one stage working on one region (and one variant, e.g.
@@ -138,7 +148,7 @@ struct StageArgs {
   int32_t use_flattening;
   int32_t use_hybrid_weno;
   int32_t weno_scheme;
-  int32_t pad;
+  int32_t umeth;  // the call is pcg_umeth (see Region::umeth)
   double difmag;
   const double* dt_dev;  // nullptr: each region's dt
   double* partial;       // fused step tail: one timestep minimum per block
@@ -154,6 +164,16 @@ struct AuxBox {
   View snew;  // S_new (may alias uin)
 };
 
+// One box of a batched ghost fill: the ghost cells of grow(domain box, ng) of its state.
+struct FillBox {
+  View state;
+  int32_t dlo[3], dhi[3];
+  int32_t periodic;  // bit d set: periodic wrap in direction d, else zero-gradient
+  int32_t pad;
+  int64_t count;     // ghost cells
+  int64_t blk0;      // first block of this box within the launch
+};
+
 struct AuxArgs {
   const AuxBox* boxes;
   const Seg* segs;
@@ -166,6 +186,11 @@ struct AuxArgs {
   View state;           // ghost fill: domain FAB
   int32_t dlo[3], dhi[3], ng, ncomp;
   int32_t periodic;     // ghost fill: bit d set when direction d is periodic
+  const FillBox* fills; // batched ghost fill
+  int32_t nfill;
+  int32_t pad;
+  const pcg::Seg* bsegs;  // per-box timestep: the advance segments of each region
+  double* dt_boxes;       // per-box timestep result (device, one per region)
 };
 
 }  // namespace pcg

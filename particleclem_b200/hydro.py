@@ -5,7 +5,9 @@ float64 tensors of shape (ncomp, nz, ny, nx) and call the native library through
 the C ABI (include/pcg_hydro.h). Names and argument meaning follow the reference:
 
 * :func:`ctoprim`       -- pc_ctoprim launch   (Source/Hydro.cpp:104-116)
+* :func:`srctoprim`     -- pc_srctoprim launch (Source/Hydro.cpp:161-174, Source/Hydro.H:14-68)
 * :func:`umdrv`         -- pc_umdrv            (Source/Hydro.H:910-935)
+* :func:`umeth`         -- pc_umeth_3D alone   (Source/Godunov.H:1142-1162)
 * :func:`hydro_box`     -- one construct_hydro_source box iteration (Source/Hydro.cpp:70-249)
 * :func:`hydro_boxes`   -- the whole box loop in one set of launches
 * :func:`estdt`         -- estTimeStep's hydro reduction (Source/PeleC.cpp:829-960)
@@ -64,6 +66,20 @@ def umdrv(prm, lo, hi, uin, uout, q, qaux, src_q, flx, area, vol, stream=None):
                 _a4p(src_q), abi.array4_list(flx), abi.array4_list(area), _a4p(vol), _stream_ptr(stream))
 
 
+def srctoprim(prm, lo, hi, q, qaux, src, srcq, stream=None):
+    """pc_srctoprim over [lo,hi]: srcq (QVAR comps) from the conserved sources src."""
+    native.call("pcg_srctoprim", C.byref(prm), abi.ivec(lo), abi.ivec(hi), _a4p(q), _a4p(qaux), _a4p(src),
+                _a4p(srcq), _stream_ptr(stream))
+
+
+def umeth(prm, lo, hi, q, qaux, src_q, flx, qec, area, pdivu, vol, stream=None):
+    """pc_umeth_3D: the unadjusted final fluxes flx[3], the face states qec[3] (NGDNV
+    components, GDRHO not written) and pdivu of box [lo,hi]."""
+    native.call("pcg_umeth", C.byref(prm), abi.ivec(lo), abi.ivec(hi), _a4p(q), _a4p(qaux), _a4p(src_q),
+                abi.array4_list(flx), abi.array4_list(qec), abi.array4_list(area), _a4p(pdivu), _a4p(vol),
+                _stream_ptr(stream))
+
+
 def hydro_box(prm, lo, hi, uin, uout, flx=None, stream=None):
     native.call("pcg_hydro_box", C.byref(prm), abi.ivec(lo), abi.ivec(hi), _a4p(uin), _a4p(uout),
                 abi.array4_list(flx) if flx is not None else None, _stream_ptr(stream))
@@ -81,7 +97,8 @@ def make_box(lo, hi, uin, uout, dx, dt, domlo=None, domhi=None, bclo=(0, 0, 0), 
     b.dx[:] = [float(v) for v in dx]
     b.dt = float(dt)
     b.uin = abi.array4(uin)
-    b.uout = abi.array4(uout)
+    if uout is not None:  # pcg_step_boxes stores no hydro source
+        b.uout = abi.array4(uout)
     if flx is not None:
         for d in range(3):
             b.flx[d] = abi.array4(flx[d])
@@ -99,6 +116,16 @@ def box_array(boxes):
 def hydro_boxes(prm, boxes, stream=None):
     arr = box_array(boxes)
     native.call("pcg_hydro_boxes", C.byref(prm), len(boxes), arr, _stream_ptr(stream))
+
+
+def step_boxes(prm, boxes, cfl, dt, dt_next, fill_ghosts=True, stream=None):
+    """One full step of independent patches (ghost fill, hydro, S_new with computeTemp in
+    place, next CFL timestep per box). dt / dt_next: CUDA float64 tensors of len(boxes)
+    (dt None: each box's own dt)."""
+    arr = box_array(boxes)
+    native.call("pcg_step_boxes", C.byref(prm), len(boxes), arr, int(bool(fill_ghosts)), float(cfl),
+                C.c_void_p(dt.data_ptr()) if dt is not None else None, C.c_void_p(dt_next.data_ptr()),
+                _stream_ptr(stream))
 
 
 def workspace_bytes(prm, extents):

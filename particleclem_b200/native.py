@@ -55,8 +55,11 @@ SIGNATURES = {
     "pcg_set_eos_nasa7": ([C.c_int, _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(C.c_double)], C.c_int),
     "pcg_ctoprim": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),
     "pcg_umdrv": ([_PRM, _I3, _I3, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _V], C.c_int),
+    "pcg_srctoprim": ([_PRM, _I3, _I3, _A4, _A4, _A4, _A4, _V], C.c_int),
+    "pcg_umeth": ([_PRM, _I3, _I3, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _V], C.c_int),
     "pcg_hydro_box": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),
     "pcg_hydro_boxes": ([_PRM, C.c_int32, _P(Box), _V], C.c_int),
+    "pcg_step_boxes": ([_PRM, C.c_int32, _P(Box), C.c_int32, C.c_double, _V, _V, _V], C.c_int),
     "pcg_hydro_workspace": ([_PRM, C.c_int32, _P(C.c_int32), _P(C.c_int32), _P(C.c_int64)], C.c_int),
     "pcg_trim_workspace": ([C.c_int32, C.c_int64], C.c_int),
     "pcg_hydro_box_noalloc": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),

@@ -12,10 +12,11 @@
                                             an inflow low-z face (low-order boundary fluxes),
                                             and the 32^3 Sod box: FP64 and mixed step times,
                                             mixed error
-  python -m particleclem_b200.suite serve   16 ensemble runs submitting flame boxes with
-                                            edges in {16,24,32,48,64}: saturated throughput
-                                            and p50/p99 latency under Poisson arrivals at
-                                            10..100 % of it, HBM admission budget
+  python -m particleclem_b200.suite serve   16 ensemble runs of flame patches with edges in
+                                            {16,24,32,48,64}, each request one step of a patch
+                                            (states evolve and stay resident): saturated
+                                            throughput and p50/p99 latency under Poisson
+                                            arrivals at 10..100 % of it, HBM admission budget
 
 Each prints one JSON line per result. All inputs are synthetic (seeded generators of
 particleclem_b200.workloads). The plain FP64 form is bit-identical to the CPU
@@ -165,44 +166,16 @@ def run_sweep(args):
 
 
 def run_serve(args):
-    import torch
+    from .serve import ensemble_serving
 
-    from .serve import GpuExecutor, Scheduler, serve_sweep
-
-    eos = wl.load_nasa7()
-    patches, runs = wl.serving_patches(nruns=args.runs, per_run=args.per_run, seed=5, eos=eos)
-    budget = int(args.budget_gb * 1e9)
-    ex = GpuExecutor(eos, precision=abi.PREC_MIXED)
-    pids = [ex.add_patch(p) for p in patches]
-    # warm the library and the stream-ordered memory pool
-    ex.start()
-    Scheduler(ex, budget).run([ex.request(k, p, 0.0) for k, p in enumerate(pids[:8])])
-    ex.synchronize()
-    res = serve_sweep(ex, pids, budget, loads=tuple(args.loads))
-    # mixed-precision error of the served hydro sources against the plain FP64 form
-    ex64 = GpuExecutor(eos, precision=abi.PREC_FP64)
-    sample = pids[: args.error_sample]
-    for k in sample:
-        ex64.add_patch(patches[k])
-    ex64.start()
-    Scheduler(ex64, budget).run([ex64.request(i, i, 0.0) for i in range(len(sample))])
-    ex64.synchronize()
-    worst_src, worst_state = 0.0, 0.0
-    g = abi.NGROW
-    for i, k in enumerate(sample):
-        # same dt for both forms (each patch's estTimeStep is FP64 in both)
-        l1, _ = _rel(torch, ex64.outs[i].data, ex.outs[k].data)
-        worst_src = max(worst_src, float(l1.max()))
-        dt = ex64.boxes[i].dt
-        s_old = ex64.states[i].data[:, g:-g, g:-g, g:-g]
-        l1s, _ = _rel(torch, s_old + dt * ex64.outs[i].data, s_old + dt * ex.outs[k].data)
-        worst_state = max(worst_state, float(l1s.max()))
-    for r in res:
-        r.update({"workload": f"serving_{args.runs}runs_x{args.per_run}_flame_boxes_16-64_ns9",
-                  "budget_gb": args.budget_gb, "precision": "mixed"})
+    out = ensemble_serving(wl.load_nasa7(), nruns=args.runs, per_run=args.per_run, nreq=args.requests,
+                           budget_bytes=int(args.budget_gb * 1e9), loads=tuple(args.loads),
+                           max_batch_cells=args.max_batch_cells, error_sample=args.error_sample)
+    for r in out["points"]:
+        r.update({"workload": out["workload"], "budget_gb": args.budget_gb, "precision": "mixed"})
         print(json.dumps(r), flush=True)
-    print(json.dumps({"serving_error_mixed_vs_fp64": {"sample": len(sample), "s_new_max_rel_l1": worst_state,
-                                                      "hydro_source_max_rel_l1": worst_src}}), flush=True)
+    print(json.dumps({"serving_error_mixed_vs_fp64": out["error_vs_fp64_one_step"],
+                      "resident_state_gb": out["resident_state_gb"]}), flush=True)
 
 
 def run_options(args):
@@ -259,7 +232,9 @@ def main(argv=None):
     v.add_argument("--runs", type=int, default=16)
     v.add_argument("--per-run", type=int, default=32)
     v.add_argument("--budget-gb", type=float, default=120.0)
-    v.add_argument("--loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.9, 1.0])
+    v.add_argument("--loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0])
+    v.add_argument("--requests", type=int, default=5000, help="step requests per load point")
+    v.add_argument("--max-batch-cells", type=int, default=2_000_000)
     v.add_argument("--error-sample", type=int, default=32)
     o = sub.add_parser("options")
     o.add_argument("--n", type=int, default=128)

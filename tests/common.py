@@ -95,3 +95,18 @@ def rel_err(got, ref):
     """(max over components of rel L1, max over components of rel Linf)."""
     l1, linf = rel_errors(got, ref)
     return float(l1.max()), float(linf.max())
+
+
+def random_sources(fab, seed, scale=2.0):
+    """A source FAB for the state ``fab`` (NVAR components on the same cells): each
+    component a smooth random field of amplitude ``scale`` times the component's typical
+    magnitude per unit time, so that hdt * srcQ perturbs the traced states by a fraction
+    of a percent at CFL-limited timesteps. The role of PeleC's sources_for_hydro
+    (Source/Hydro.cpp:29-46) in a run with reactions or diffusion."""
+    rng = np.random.default_rng(seed)
+    u = fab.data
+    out = np.empty_like(u)
+    for n in range(u.shape[0]):
+        mag = np.abs(u[n]).mean() + 1e-30
+        out[n] = scale * mag * wl._smooth_noise(rng, u.shape[1:])
+    return abi.Fab(out, tuple(fab.lo))

@@ -91,3 +91,40 @@ def test_oracle_equals_reference_build_hybrid_weno(scheme, nspec, seed):
     prm.use_hybrid_weno = 0
     c, _ = o.hydro_box(prm, p.lo, p.hi, p.fab)
     assert not np.array_equal(a.data, c.data)  # the WENO branch was taken
+
+
+@pytest.mark.parametrize("nspec", [1, 9])
+@pytest.mark.parametrize("ppm", [1, 0])
+def test_oracle_equals_reference_build_srctoprim_and_umeth_with_sources(nspec, ppm):
+    """pc_srctoprim (Source/Hydro.H:14-68) of non-zero sources, then pc_umeth_3D
+    (Source/Godunov.cpp:59-476) with those primitive sources, so that the hdt * srcQ terms
+    of pc_transdd (Source/Godunov.H:639-845) are taken: final fluxes, the face states qec
+    (components GDU..GDGAME) and p div u agree bit for bit, and pc_umdrv with the same
+    srcQ too."""
+    if not pyoracle.ref_available(nspec):
+        pytest.skip("oracle/_ref not built (needs the reference checkout)")
+    from common import random_sources
+
+    eos = wl.GammaLaw() if nspec == 1 else eos9()
+    p = wl.random_patch((6, 5, 4), 611 + nspec, eos if nspec == 9 else None)
+    ref = pyoracle.reference(nspec)
+    ref.set_eos(eos)
+    o = oracle()
+    o.set_eos(eos)
+    g4lo, g4hi = abi.grow(p.lo, p.hi, 4)
+    dt = 0.3 * ref.estdt(p.lo, p.hi, p.fab, p.dx)
+    prm = abi.make_params(p.dx, dt, nspec, (-BIG,) * 3, (BIG,) * 3, (0, 0, 0), (0, 0, 0), ppm_type=ppm)
+    q, qa = ref.ctoprim(g4lo, g4hi, p.fab)
+    src = random_sources(p.fab, 7 + nspec, scale=20.0 if nspec == 1 else 1e4)
+    sq_ref = ref.srctoprim(g4lo, g4hi, q, qa, src)
+    sq_orc = o.srctoprim(g4lo, g4hi, q, qa, src)
+    np.testing.assert_array_equal(sq_orc.data, sq_ref.data)
+    assert np.abs(sq_ref.data).max() > 0
+    fa, ga, pa = o.umeth(prm, p.lo, p.hi, q, qa, sq_orc)
+    fb, gb, pb = ref.umeth(prm, p.lo, p.hi, q, qa, sq_ref)
+    for d in range(3):
+        np.testing.assert_array_equal(fa[d].data, fb[d].data)
+        np.testing.assert_array_equal(ga[d].data[1:], gb[d].data[1:])
+    np.testing.assert_array_equal(pa.data, pb.data)
+    f0, _, _ = o.umeth(prm, p.lo, p.hi, q, qa, None)
+    assert not np.array_equal(f0[0].data, fa[0].data)  # the sources entered the fluxes

@@ -20,11 +20,15 @@ class SimExecutor:
         self.busy_until = 0.0
         self.finishes = []
         self.batches = []
+        self.evicted = []
+
+    def evict(self, pid):
+        self.evicted.append(pid)
 
     def now(self):
         return self.t
 
-    def launch(self, batch):
+    def launch(self, batch, slot=0):
         start = max(self.t, self.busy_until)
         fin = start + self.overhead + self.per_cell * sum(r.cells for r in batch)
         self.busy_until = fin
@@ -125,3 +129,35 @@ def test_workspace_query_is_host_only_and_additive():
     d = hydro.workspace_bytes(abi.make_params((1, 1, 1), 0.0, 9, (0,) * 3, (0,) * 3, (0,) * 3, (0,) * 3,
                                               precision_mode=abi.PREC_FP64), [((0, 0, 0), (31, 31, 31))])
     assert m < d
+
+
+def test_steps_of_one_patch_stay_in_order():
+    """Two requests for the same patch never share a batch and the second starts after
+    the first has finished (each step reads the state the previous one wrote)."""
+    reqs = [Request(0, 7, 0.0, cells=1000, nbytes=1), Request(1, 3, 0.0, cells=1000, nbytes=1),
+            Request(2, 7, 0.0, cells=1000, nbytes=1)]
+    sch = Scheduler(SimExecutor(), budget_bytes=100, max_inflight=2)
+    sch.run(reqs)
+    assert reqs[0].batch != reqs[2].batch
+    assert reqs[2].start >= reqs[0].finish
+
+
+def test_resident_states_are_evicted_least_recently_used_within_the_budget():
+    """Four patches whose states take 40 bytes each (workspace 10) under a budget of 100:
+    at most two states fit beside a step's workspace, so idle states are evicted, least
+    recently used first, and the budget holds throughout."""
+    ex = SimExecutor()
+    pids = [0, 1, 2, 3, 0, 1, 2, 3]
+    reqs = [Request(k, p, 1e-3 * k, cells=1000, nbytes=10, state_bytes=40) for k, p in enumerate(pids)]
+    sch = Scheduler(ex, budget_bytes=100, max_inflight=1)
+    sch.run(reqs)
+    assert sch.peak_bytes <= 100
+    assert ex.evicted[:2] == [0, 1]  # patch 2 evicts 0, patch 3 evicts 1
+    assert sch.evictions == len(ex.evicted) and sch.uploads == 4 + sch.evictions - (4 - len(sch.resident))
+
+
+def test_max_batch_cells():
+    reqs = [Request(k, k, 0.0, cells=1000, nbytes=1) for k in range(10)]
+    ex = SimExecutor()
+    Scheduler(ex, budget_bytes=100, max_inflight=2, max_batch_cells=2500).run(reqs)
+    assert [len(b) for b in ex.batches] == [2, 2, 2, 2, 2]

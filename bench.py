@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=5000, help="step requests per serving load point")
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0])
     ap.add_argument("--serve-batch-cells", type=int, default=2_000_000, help="cells per serving batch at most")
+    ap.add_argument("--sweep-steps", type=int, default=100, help="steps of the precision sweep")
+    ap.add_argument("--no-side-workloads", action="store_true",
+                    help="skip the batching and precision-sweep workloads (quick runs)")
     ap.add_argument("--cpu-configs", action="store_true",
                     help="only time the CPU baseline on the Sod box, the flame level and the turbulence level "
                          "(PPM and PLM), one JSON line each")
@@ -498,6 +501,16 @@ def run_ours(args):
                                budget_bytes=int(120e9), loads=tuple(args.serve_loads),
                                max_batch_cells=args.serve_batch_cells, error_sample=32, device=local)
 
+    # ---- batching (512 independent flame boxes, edges log-uniform in [8, 64]) and the
+    # precision sweep (256^3 periodic turbulence as 64 boxes of 64^3, PPM and PLM): mixed
+    # against the plain FP64 form, step times in CUDA graphs and errors
+    from particleclem_b200.suite import batch_workload, sweep_workload
+
+    batching = sweep = None
+    if not args.no_side_workloads:
+        batching = batch_workload(512, steps=5, warmup=3, device=local)
+        sweep = sweep_workload(256, 64, steps=args.sweep_steps, every=10, device=local)
+
     # ---- roofline: the dominant kernel (one fused region of the whole level) and the step
     from particleclem_b200 import roofline as rl
 
@@ -545,6 +558,8 @@ def run_ours(args):
                                                      "batches", "peak_bytes")}
                                   for r in serving["points"][1:]],
                         "error_vs_fp64_one_step": serving["error_vs_fp64_one_step"]},
+            "batching": batching,
+            "precision_sweep": sweep,
             "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 1, stages 6, fused tail 1, final dt 1
             "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},

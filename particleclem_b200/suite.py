@@ -18,6 +18,9 @@
                                             throughput and p50/p99 latency under Poisson
                                             arrivals at 10..100 % of it, HBM admission budget
 
+  python -m particleclem_b200.suite step    a few eager steps of one level in one form (the
+                                            workload of the kernel profiles)
+
 Each prints one JSON line per result. All inputs are synthetic (seeded generators of
 particleclem_b200.workloads). The plain FP64 form is bit-identical to the CPU
 restatement of the reference (the GPU parity tests), so errors against it are errors
@@ -77,13 +80,17 @@ def _rel(torch, a, b):
     return l1, li
 
 
-def run_batch(args):
+def batch_workload(nbox=512, steps=10, warmup=3, device=0):
+    """The batching workload: ``nbox`` independent flame boxes with edges log-uniform in
+    [8, 64] per axis (9 species), one plan over all boxes, one CUDA graph per step; mixed
+    and plain FP64 step times and the error of one mixed step against the FP64 one
+    (group-normalised relative L1 / Linf of S_new)."""
     import torch
 
     from .batch import BoxBatch
 
     eos = wl.load_nasa7()
-    patches = wl.flame_boxes(args.nbox, seed=3, eos=eos, lo=8, hi=64)
+    patches = wl.flame_boxes(nbox, seed=3, eos=eos, lo=8, hi=64)
     ncell = sum(p.ncells for p in patches)
     pk = rl.peaks(ROOT)
     edges = [[p.hi[d] - p.lo[d] + 1 for d in range(3)] for p in patches]
@@ -92,56 +99,58 @@ def run_batch(args):
     states = {}
     launches = None
     for name, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
-        bb = BoxBatch(patches, eos, precision=prec)
+        bb = BoxBatch(patches, eos, precision=prec, device=device)
         bb.step()  # one step from the initial state, kept for the error
         torch.cuda.synchronize()
         states[name] = [s.data.clone() for s in bb.states]
         bb.capture()
         launches = bb.launches_per_step
-        ms = _timed(torch, bb.replay, args.steps, args.warmup)
+        ms = _timed(torch, bb.replay, steps, warmup)
         res[name] = {"ms_per_step": ms, "cell_updates_per_s": ncell / (ms / 1e3),
                      "path_hbm_frac": balg / (ms / 1e3) / 1e9 / pk["hbm_gbs"]}
         bb.close()
         del bb
         torch.cuda.empty_cache()
     g = abi.NGROW
-    num = torch.zeros(abi.nvar(9), dtype=torch.float64, device="cuda")
-    den = torch.zeros_like(num)
-    mx_d = torch.zeros_like(num)
-    mx_r = torch.zeros_like(num)
-    for a, b in zip(states["fp64"], states["mixed"]):
-        a = a[:, g:-g, g:-g, g:-g].reshape(a.shape[0], -1)
-        b = b[:, g:-g, g:-g, g:-g].reshape(b.shape[0], -1)
-        num += (a - b).abs().sum(1)
-        den += a.abs().sum(1)
-        mx_d = torch.maximum(mx_d, (a - b).abs().max(1).values)
-        mx_r = torch.maximum(mx_r, a.abs().max(1).values)
-    l1 = (num / den.clamp_min(1e-300)).cpu().numpy()
-    li = (mx_d / mx_r.clamp_min(1e-300)).cpu().numpy()
-    out = {"workload": f"flame_boxes_{args.nbox}_loguniform_8_64_ns9", "boxes": args.nbox, "cells": ncell,
-           "mixed": res["mixed"], "fp64": res["fp64"], "speedup_mixed_over_fp64": res["fp64"]["ms_per_step"] /
-           res["mixed"]["ms_per_step"], "error_mixed_vs_fp64_one_step": {"max_rel_l1": float(l1.max()),
-                                                                        "max_rel_linf": float(li.max())},
-           "launches_per_step": launches, "b_alg_bytes_per_step": balg, "peak_source": pk["source"]}
-    print(json.dumps(out), flush=True)
+    a = torch.cat([x[:, g:-g, g:-g, g:-g].reshape(x.shape[0], -1) for x in states["fp64"]], dim=1)
+    b = torch.cat([x[:, g:-g, g:-g, g:-g].reshape(x.shape[0], -1) for x in states["mixed"]], dim=1)
+    l1, li = _rel_grouped(torch, a, b, 9)
+    return {"workload": f"flame_boxes_{nbox}_loguniform_8_64_ns9", "boxes": nbox, "cells": ncell,
+            "mixed": res["mixed"], "fp64": res["fp64"],
+            "speedup_mixed_over_fp64": res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"],
+            "error_mixed_vs_fp64_one_step": {"s_new_max_rel_l1": float(l1.max()), "s_new_max_rel_linf": float(li.max()),
+                                             "normalisation": "per physical group"},
+            "launches_per_step": launches, "b_alg_bytes_per_step": balg, "peak_source": pk["source"]}
 
 
-def run_sweep(args):
+def run_batch(args):
+    print(json.dumps(batch_workload(args.nbox, args.steps, args.warmup)), flush=True)
+
+
+def sweep_workload(n=256, box=64, steps=100, every=10, schemes=(1, 0), device=0):
+    """The precision sweep: the periodic decaying-turbulence level (gamma law), PPM
+    (scheme 1) and PLM (0), plain FP64 per box against mixed fused, step times (CUDA graphs)
+    and the error growth of the mixed state against the FP64 one over ``steps`` steps taken
+    with the FP64 run's timestep sequence (so the difference is precision only)."""
     import torch
 
     from .level import LevelStepper
 
-    lev0 = wl.turbulence(n=args.n, box=args.box, seed=4)
-    for ppm in (1, 0):
-        a = LevelStepper(lev0, precision=abi.PREC_FP64, fuse=False, ppm_type=ppm)
-        b = LevelStepper(lev0, precision=abi.PREC_MIXED, fuse=True, ppm_type=ppm)
-        ms_a = _timed(torch, a.step, 3, 1)
-        ms_b = _timed(torch, b.step, 3, 1)
+    lev0 = wl.turbulence(n=n, box=box, seed=4)
+    out = []
+    for ppm in schemes:
+        a = LevelStepper(lev0, precision=abi.PREC_FP64, fuse=False, ppm_type=ppm, device=device)
+        b = LevelStepper(lev0, precision=abi.PREC_MIXED, fuse=True, ppm_type=ppm, device=device)
+        a.capture()
+        b.capture()
+        ms_a = _timed(torch, a.replay, 3, 2)
+        ms_b = _timed(torch, b.replay, 3, 2)
+        a.graph = b.graph = None
         a.state.data.copy_(torch.from_numpy(lev0.state).to(a.dev))
         b.state.data.copy_(a.state.data)
         growth = []
         g = abi.NGROW
-        for s in range(1, args.steps + 1):
+        for s in range(1, steps + 1):
             a.fill()
             a.plan.estdt(a.cfl, a.dt)
             a.plan.hydro(a.dt)
@@ -150,19 +159,25 @@ def run_sweep(args):
             b.dt.copy_(a.dt)  # the same timestep sequence: the difference is precision only
             b.plan.hydro(b.dt)
             b.plan.update(b.dt)
-            if s in (1, 2, 5) or s % args.every == 0:
-                l1, li = _rel(torch, a.state.data[:, g:-g, g:-g, g:-g], b.state.data[:, g:-g, g:-g, g:-g])
+            if s in (1, 2, 5) or s % every == 0:
+                l1, li = _rel_grouped(torch, a.state.data[:, g:-g, g:-g, g:-g], b.state.data[:, g:-g, g:-g, g:-g], 1)
                 growth.append({"step": s, "max_rel_l1": float(l1[:5].max()), "max_rel_linf": float(li[:5].max())})
-        out = {"workload": f"turbulence_{args.n}^3_as_{args.box}^3_boxes_ns1_mach0.3", "scheme": "PPM" if ppm else "PLM",
-               "fp64_ms_per_step": ms_a, "mixed_ms_per_step": ms_b,
-               "fp64_cell_updates_per_s": lev0.ncells() / (ms_a / 1e3),
-               "mixed_cell_updates_per_s": lev0.ncells() / (ms_b / 1e3),
-               "error_components": "rho, rho u, rho v, rho w, rho E", "growth": growth}
-        print(json.dumps(out), flush=True)
+        out.append({"workload": f"turbulence_{n}^3_as_{box}^3_boxes_ns1_mach0.3", "scheme": "PPM" if ppm else "PLM",
+                    "fp64_ms_per_step": ms_a, "mixed_ms_per_step": ms_b,
+                    "fp64_cell_updates_per_s": lev0.ncells() / (ms_a / 1e3),
+                    "mixed_cell_updates_per_s": lev0.ncells() / (ms_b / 1e3),
+                    "speedup_mixed_over_fp64": ms_a / ms_b,
+                    "error_components": "rho, rho u, rho v, rho w, rho E (per physical group)", "growth": growth})
         a.close()
         b.close()
         del a, b
         torch.cuda.empty_cache()
+    return out
+
+
+def run_sweep(args):
+    for r in sweep_workload(args.n, args.box, args.steps, args.every):
+        print(json.dumps(r), flush=True)
 
 
 def run_serve(args):
@@ -216,6 +231,24 @@ def run_options(args):
         del states
 
 
+def run_step(args):
+    """A few eager steps of one level (the profiling workload): the flame level of edge n
+    (9 species) or the turbulence level (one species), one form."""
+    import torch
+
+    from .level import LevelStepper
+
+    lev = wl.flame(n=args.n, box=args.box, seed=2) if args.level == "flame" else wl.turbulence(n=args.n, box=args.box)
+    prec = {"mixed": abi.PREC_MIXED, "fp64": abi.PREC_FP64, "fast": abi.PREC_FP64_FAST}[args.form]
+    st = LevelStepper(lev, precision=prec, fuse=not args.per_box, ppm_type=args.ppm)
+    for _ in range(args.steps):
+        st.step()
+    torch.cuda.synchronize()
+    print(json.dumps({"level": args.level, "n": args.n, "form": args.form, "steps": args.steps,
+                      "dt": float(st.dt.item())}), flush=True)
+    st.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -236,13 +269,22 @@ def main(argv=None):
     v.add_argument("--requests", type=int, default=5000, help="step requests per load point")
     v.add_argument("--max-batch-cells", type=int, default=2_000_000)
     v.add_argument("--error-sample", type=int, default=32)
+    t = sub.add_parser("step")
+    t.add_argument("--level", choices=("flame", "turbulence"), default="flame")
+    t.add_argument("--n", type=int, default=64)
+    t.add_argument("--box", type=int, default=32)
+    t.add_argument("--form", choices=("mixed", "fp64", "fast"), default="mixed")
+    t.add_argument("--ppm", type=int, default=1)
+    t.add_argument("--per-box", action="store_true", help="advance the boxes as separate regions")
+    t.add_argument("--steps", type=int, default=2)
     o = sub.add_parser("options")
     o.add_argument("--n", type=int, default=128)
     o.add_argument("--box", type=int, default=32)
     o.add_argument("--steps", type=int, default=10)
     o.add_argument("--warmup", type=int, default=3)
     args = ap.parse_args(argv)
-    {"batch": run_batch, "sweep": run_sweep, "serve": run_serve, "options": run_options}[args.cmd](args)
+    {"batch": run_batch, "sweep": run_sweep, "serve": run_serve, "options": run_options,
+     "step": run_step}[args.cmd](args)
     return 0
 
 

@@ -24,6 +24,7 @@ Workloads (sizes as named by the benchmark configurations):
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -323,10 +324,31 @@ def log_uniform_edges(nbox, seed, lo=8, hi=64):
     return np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), size=(nbox, 3)))).astype(int)
 
 
-def flame_boxes(nbox=512, seed=3, eos=None, lo=8, hi=64):
+def _flame_patch_job(spec):
+    edges, seed, eos = spec
+    return flame_patch(edges, seed, eos)
+
+
+def flame_patches(specs, eos=None, workers=None):
+    """flame_patch for every (edges, seed) of ``specs``, in order. Many patches are
+    generated in parallel by a pool of worker processes started with "spawn" (no CUDA
+    state is inherited), each patch from its own seed, so the result is the same as the
+    serial one."""
     eos = eos or load_nasa7()
+    workers = min(16, os.cpu_count() or 1) if workers is None else int(workers)
+    if workers <= 1 or len(specs) < 16:
+        return [flame_patch(e, sd, eos) for e, sd in specs]
+    import multiprocessing
+    from concurrent.futures import ProcessPoolExecutor
+
+    with ProcessPoolExecutor(max_workers=workers, mp_context=multiprocessing.get_context("spawn")) as ex:
+        return list(ex.map(_flame_patch_job, [(tuple(int(x) for x in e), int(sd), eos) for e, sd in specs],
+                           chunksize=max(1, len(specs) // (4 * workers))))
+
+
+def flame_boxes(nbox=512, seed=3, eos=None, lo=8, hi=64):
     edges = log_uniform_edges(nbox, seed, lo, hi)
-    return [flame_patch(e, seed * 100003 + b, eos) for b, e in enumerate(edges)]
+    return flame_patches([(e, seed * 100003 + b) for b, e in enumerate(edges)], eos)
 
 
 def serving_patches(nruns=16, per_run=32, seed=5, eos=None, edges=(16, 24, 32, 48, 64)):
@@ -334,15 +356,14 @@ def serving_patches(nruns=16, per_run=32, seed=5, eos=None, edges=(16, 24, 32, 4
     boxes whose edges are drawn uniformly from ``edges`` per axis (run-seeded), each
     with its own front offset. Returned in submission order (runs interleaved) with
     the run of each."""
-    eos = eos or load_nasa7()
     rngs = [np.random.default_rng(seed * 1000 + r) for r in range(nruns)]
-    patches, runs = [], []
+    specs, runs = [], []
     for k in range(per_run):
         for r in range(nruns):
             e = rngs[r].choice(np.asarray(edges), size=3)
-            patches.append(flame_patch(e, seed * 100003 + r * 1009 + k, eos))
+            specs.append((e, seed * 100003 + r * 1009 + k))
             runs.append(r)
-    return patches, runs
+    return flame_patches(specs, eos), runs
 
 
 # ------------------------------------------------------------------ turbulence (config 4)
@@ -350,7 +371,8 @@ def turbulence(n=256, box=64, seed=4, kmax=32, mach=0.3, gamma=1.4) -> Level:
     eos = GammaLaw(gamma=gamma)
     rng = np.random.default_rng(seed)
     k = np.fft.fftfreq(n, d=1.0 / n)
-    KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
+    # wavenumber components broadcast over (kz, ky, kx) instead of full meshgrid copies
+    KZ, KY, KX = k[:, None, None], k[None, :, None], k[None, None, :]
     K = np.sqrt(KX * KX + KY * KY + KZ * KZ)
     shell = (K >= 0.5) & (K <= kmax + 0.5)
     amp = np.zeros_like(K)
@@ -359,7 +381,8 @@ def turbulence(n=256, box=64, seed=4, kmax=32, mach=0.3, gamma=1.4) -> Level:
     uh = []
     for _ in range(3):
         ph = rng.uniform(0, 2 * np.pi, size=K.shape)
-        uh.append(amp * np.exp(1j * ph))
+        # exp(i ph) as cos + i sin: the same values, several times faster than complex exp
+        uh.append(amp * (np.cos(ph) + 1j * np.sin(ph)))
     Ksafe = np.where(K == 0, 1.0, K)
     kdotu = (KX * uh[0] + KY * uh[1] + KZ * uh[2]) / (Ksafe ** 2)
     uh = [uh[0] - KX * kdotu, uh[1] - KY * kdotu, uh[2] - KZ * kdotu]  # solenoidal projection

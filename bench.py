@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--serve-batch-cells", type=int, default=2_000_000, help="cells per serving batch at most")
     ap.add_argument("--sweep-steps", type=int, default=100, help="steps of the precision sweep")
     ap.add_argument("--no-side-workloads", action="store_true",
-                    help="skip the batching and precision-sweep workloads (quick runs)")
+                    help="skip the batching, precision-sweep and serving workloads (quick runs)")
     ap.add_argument("--cpu-configs", action="store_true",
                     help="only time the CPU baseline on the Sod box, the flame level and the turbulence level "
                          "(PPM and PLM), one JSON line each")
@@ -367,6 +367,23 @@ def run_ours(args):
         e2e_value = e2e_serial = world * ncell * kp / (mse / 1e3)
         lev = wl.flame(n=args.n, box=args.box, seed=2 + rank)  # per-GPU level for the side measurements
 
+    # ---- fixed cost of the step's launch sequence: the same CUDA graph (ghost fill, 6
+    # hydro stages, fused tail, final minimum) on an 8^3 level, whose kernels do almost no
+    # work; it bounds what merging the launches into one persistent kernel could save
+    tiny = LevelStepper(wl.flame(n=8, box=8, seed=2), precision=abi.PREC_MIXED, fuse=True, device=local)
+    tiny.capture()
+    for _ in range(20):
+        tiny.replay()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(200):
+        tiny.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    graph_overhead = {"workload": "flame level 8^3, one box", "launches": LevelStepper.launches_per_step,
+                      "ms_per_step": e0.elapsed_time(e1) / 200}
+    tiny.close()
+
     # ---- per-stage CUDA-event timings of the same step (not graph-captured)
     # "advance" is the launch sequence the level step uses: the hydro stages up to flux2,
     # then flux divergence + update + computeTemp + next CFL minimum in one pass
@@ -497,9 +514,11 @@ def run_ours(args):
     # a resident, evolving patch; HBM budget 120 GB; two streams)
     from particleclem_b200.serve import ensemble_serving
 
-    serving = ensemble_serving(lev.eos, nruns=16, per_run=32, seed=5 + rank, nreq=args.serve_requests,
-                               budget_bytes=int(120e9), loads=tuple(args.serve_loads),
-                               max_batch_cells=args.serve_batch_cells, error_sample=32, device=local)
+    serving = None
+    if not args.no_side_workloads:
+        serving = ensemble_serving(lev.eos, nruns=16, per_run=32, seed=5 + rank, nreq=args.serve_requests,
+                                   budget_bytes=int(120e9), loads=tuple(args.serve_loads),
+                                   max_batch_cells=args.serve_batch_cells, error_sample=32, device=local)
 
     # ---- batching (512 independent flame boxes, edges log-uniform in [8, 64]) and the
     # precision sweep (256^3 periodic turbulence as 64 boxes of 64^3, PPM and PLM): mixed
@@ -549,7 +568,7 @@ def run_ours(args):
                             "-> D2H, every step",
                     "serial": {"value": e2e_serial, "ms_per_step": mse_serial / ke,
                                "path": "same copies and step, one after another"}},
-            "serving": {"workload": serving["workload"], "budget_gb": serving["budget_gb"],
+            "serving": None if serving is None else {"workload": serving["workload"], "budget_gb": serving["budget_gb"],
                         "max_batch_cells": serving["max_batch_cells"],
                         "resident_state_gb": serving["resident_state_gb"],
                         "saturated_cell_updates_per_s": serving["points"][0]["cell_updates_per_s"],
@@ -558,6 +577,7 @@ def run_ours(args):
                                                      "batches", "peak_bytes")}
                                   for r in serving["points"][1:]],
                         "error_vs_fp64_one_step": serving["error_vs_fp64_one_step"]},
+            "graph_step_overhead": graph_overhead,
             "batching": batching,
             "precision_sweep": sweep,
             "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 1, stages 6, fused tail 1, final dt 1

@@ -230,7 +230,8 @@ int pcg_fill_ghosts(const pcg_array4* state, const int32_t domlo[3], const int32
 /* Copy the cells [lo, hi] of every component from src to dst, two arrays of equal
  * component count whose rows are contiguous (kstride a multiple of jstride); either may
  * be host or device memory (unified addressing tells which; pinned host memory for an
- * asynchronous copy). One strided copy per component, enqueued on stream. This moves a
+ * asynchronous copy). Between two arrays on one device: one kernel over all components;
+ * otherwise one strided copy per component. Enqueued on stream. This moves a
  * level's valid cells between a host FAB and the device FAB whose ghost cells
  * pcg_fill_ghosts forms, so ghost cells do not cross the bus. No counterpart in the
  * reference (AMReX moves a MultiFab's valid region with its own copy routines). */

@@ -7,22 +7,23 @@
 
 namespace PCG_TU {
 
-enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES };
+enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES, AUX_COPY };
 
 __device__ __forceinline__ bool aux_item(const pcg::AuxArgs& a, const pcg::AuxBox*& bx, int& i, int& j, int& k) {
-  const int64_t blk = blockIdx.x;
+  const int blk = blockIdx.x;
   int lo = 0, hi = a.nseg - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (a.segs[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
   }
   const pcg::Seg& s = a.segs[lo];
-  const int64_t local = (blk - s.blk0) * blockDim.x + threadIdx.x;
-  if (local >= s.count) return false;
-  const int64_t t = local / s.n[0];
-  i = s.lo[0] + (int)(local - t * s.n[0]);
-  j = s.lo[1] + (int)(t % s.n[1]);
-  k = s.lo[2] + (int)(t / s.n[1]);
+  const unsigned local = unsigned(blk - (int)s.blk0) * blockDim.x + threadIdx.x;
+  if (local >= (unsigned)s.count) return false;
+  const unsigned n0 = s.n[0], n1 = s.n[1];
+  const unsigned t = local / n0;
+  i = s.lo[0] + (int)(local - t * n0);
+  j = s.lo[1] + (int)(t % n1);
+  k = s.lo[2] + (int)(t / n1);
   bx = a.boxes + s.region;
   return true;
 }
@@ -236,6 +237,19 @@ __global__ void __launch_bounds__(128) k_estdt_boxes(pcg::AuxArgs a) {
   if (threadIdx.x == 0) a.dt_boxes[blockIdx.x] = v * a.cfl;
 }
 
+// Copy of the cells [dlo, dhi] of every component from one device FAB (state) to another
+// (dst), FP64: the packing and unpacking of halo planes. One thread per cell and component.
+__global__ void __launch_bounds__(128) k_copy_box(pcg::AuxArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n0 = a.dhi[0] - a.dlo[0] + 1, n1 = a.dhi[1] - a.dlo[1] + 1, n2 = a.dhi[2] - a.dlo[2] + 1;
+  const int64_t cells = n0 * n1 * n2;
+  if (t >= cells * a.ncomp) return;
+  const int comp = (int)(t / cells);
+  const int64_t c = t - comp * cells;
+  const int i = a.dlo[0] + (int)(c % n0), j = a.dlo[1] + (int)((c / n0) % n1), k = a.dlo[2] + (int)(c / (n0 * n1));
+  v4<double>(a.dst)(i, j, k, comp) = v4<const double>(a.state)(i, j, k, comp);
+}
+
 __global__ void __launch_bounds__(128) k_fill(pcg::AuxArgs a) {
   fill_ghost((int64_t)blockIdx.x * blockDim.x + threadIdx.x, a.dlo, a.dhi, a.ng, a.periodic, a.state, a.ncomp);
 }
@@ -264,6 +278,7 @@ static cudaError_t launch_aux_t(int which, const pcg::AuxArgs& a, int64_t nblock
     case AUX_FILL: k_fill<<<grid, block, 0, s>>>(a); break;
     case AUX_FILL_BOXES: k_fill_boxes<<<grid, block, 0, s>>>(a); break;
     case AUX_ESTDT_BOXES: k_estdt_boxes<<<grid, block, 0, s>>>(a); break;
+    case AUX_COPY: k_copy_box<<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

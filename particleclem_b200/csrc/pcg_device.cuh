@@ -58,18 +58,23 @@ template <class R> __device__ __forceinline__ R pfloor(R f, R p0) {
 }
 
 // ------------------------------------------------------------------ views
+// Element offsets within one view are 32-bit: the host refuses arrays whose component
+// extent (ncomp * nstride) or strides reach 2^31 elements (pcg::kMaxViewElems), so every
+// address is one 32-bit index computation and one scaled add to the 64-bit base, instead
+// of 64-bit multiply-adds per component (the flux stages' address arithmetic was about a
+// third of their instructions with 64-bit offsets).
 template <class T>
 struct V4 {
   T* p;
-  int64_t js, ks, ns;
+  int js, ks, ns;
   int bx, by, bz;
   __device__ __forceinline__ T& operator()(int i, int j, int k, int n = 0) const {
-    return p[(int64_t)(i - bx) + (int64_t)(j - by) * js + (int64_t)(k - bz) * ks + (int64_t)n * ns];
+    return p[(i - bx) + (j - by) * js + (k - bz) * ks + n * ns];
   }
 };
 template <class T>
 __device__ __forceinline__ V4<T> v4(const pcg::View& w) {
-  return V4<T>{reinterpret_cast<T*>(w.p), w.js, w.ks, w.ns, w.b[0], w.b[1], w.b[2]};
+  return V4<T>{reinterpret_cast<T*>(w.p), (int)w.js, (int)w.ks, (int)w.ns, w.b[0], w.b[1], w.b[2]};
 }
 
 // ------------------------------------------------------------------ EOS

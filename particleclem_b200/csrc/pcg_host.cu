@@ -92,7 +92,7 @@ enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NS
 // launches that are not stages of their own: the low-order inflow/user_bc faces, run as
 // part of stage K_FLUX2 right after it, and pc_srctoprim (pcg_srctoprim)
 enum { K_LOWBC = K_NSTAGE, K_SRCQ, K_NKIND };
-enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES };
+enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES, AUX_COPY };
 constexpr int kThreads = 128;
 constexpr size_t kAlign = 256;
 
@@ -251,7 +251,17 @@ bool covers(const pcg_array4* a, const IBox& b, int ncomp) {
   return a->ncomp >= ncomp;
 }
 
+// Largest element offset of an array from its begin corner (the kernels' 32-bit offsets).
+int64_t max_offset(const pcg_array4* a) {
+  return int64_t(a->end[0] - a->begin[0] - 1) + int64_t(a->end[1] - a->begin[1] - 1) * a->jstride +
+         int64_t(a->end[2] - a->begin[2] - 1) * a->kstride + int64_t(a->ncomp - 1) * a->nstride;
+}
+
 int check_array(const char* what, const pcg_array4* a, const IBox& b, int ncomp) {
+  if (a && a->p && (max_offset(a) > pcg::kMaxViewElems || a->jstride > pcg::kMaxViewElems ||
+                    a->kstride > pcg::kMaxViewElems || a->nstride > pcg::kMaxViewElems))
+    return fail(PCG_EINVAL, "%s spans more than 2^31 elements (the kernels address arrays with 32-bit offsets)",
+                what);
   if (!covers(a, b, ncomp))
     return fail(PCG_EINVAL, "%s must cover [%d,%d,%d]-[%d,%d,%d] with %d components", what, b.lo[0], b.lo[1],
                 b.lo[2], b.hi[0], b.hi[1], b.hi[2], ncomp);
@@ -298,6 +308,7 @@ struct BoxIn {
 };
 
 struct Layout {
+  bool oversize = false;  // a workspace array would span 2^31 elements or more
   int ns = 1;
   int umeth = 0;  // the plan is a pcg_umeth call
   size_t esz = 8;  // compute-type size of the intermediates
@@ -315,6 +326,7 @@ size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v) {
   v.ns = b.cells();
   for (int d = 0; d < 3; ++d) v.b[d] = b.lo[d];
   L.ws_bytes = off + size_t(b.cells()) * nc * esz;
+  if (b.cells() * nc > pcg::kMaxViewElems) L.oversize = true;
   return off;
 }
 
@@ -549,6 +561,7 @@ int run_once(const pcg_hydro_params* p, std::vector<BoxIn>& boxes, int first, in
   if (rc) return rc;
   Layout L;
   build_layout(L, boxes, p);
+  if (L.oversize) return fail(PCG_EINVAL, "a region needs workspace arrays of 2^31 elements or more: use smaller boxes");
   void* ws = nullptr;
   if (L.ws_bytes) CUDA_TRY(ws_alloc(&ws, L.ws_bytes, s));
   rebase_workspace(L, boxes, static_cast<char*>(ws));
@@ -660,7 +673,10 @@ void fuse_boxes(std::vector<BoxIn>& boxes) {
         for (int d = 0; d < 3; ++d) ov = ov && p.lo[d] <= q.hi[d] && q.lo[d] <= p.hi[d];
         disjoint = !ov;
       }
-    if (grp.size() > 1 && disjoint && vol == bb.cells()) {
+    // the merged region's largest workspace array (QVAR components on grow(region, 4))
+    // must stay addressable with 32-bit offsets
+    const bool fits = grow(bb, 4).cells() * pcg::qvar(pcg::MAXNS) <= pcg::kMaxViewElems;
+    if (grp.size() > 1 && disjoint && vol == bb.cells() && fits) {
       BoxIn M = A;
       M.bx = bb;
       out.push_back(M);
@@ -968,6 +984,7 @@ int pcg_step_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* box
     if ((rc = box_from_desc(boxes[b], nv, bs[b], false))) return rc;
   Layout L;
   build_layout(L, bs, prm);
+  if (L.oversize) return fail(PCG_EINVAL, "a region needs workspace arrays of 2^31 elements or more: use smaller boxes");
   for (int b = 0; b < nbox; ++b) L.regions[b].dt_ptr = dt ? dt + b : nullptr;
   // ghost fill table: each box is its own domain (periodic where both its boundary types
   // are interior, zero-gradient elsewhere)
@@ -1064,6 +1081,7 @@ int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t
   }
   Layout L;
   build_layout(L, bs, prm);
+  if (L.oversize) return fail(PCG_EINVAL, "a region needs workspace arrays of 2^31 elements or more: use smaller boxes");
   Tables T;
   pack_tables(L, T);
   *bytes = int64_t((L.ws_bytes + kAlign - 1) / kAlign * kAlign + T.bytes);
@@ -1194,6 +1212,24 @@ int pcg_copy_cells(const pcg_array4* src, const pcg_array4* dst, const int32_t l
     if (a->jstride < a->end[0] - a->begin[0] || a->kstride % a->jstride || a->kstride / a->jstride < a->end[1] - a->begin[1])
       return fail(PCG_EINVAL, "array rows must be contiguous with kstride a multiple of jstride");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // Both arrays in device memory: one kernel over all components (the packing and
+  // unpacking of halo planes inside a captured step)
+  cudaPointerAttributes pa{}, pb{};
+  if (cudaPointerGetAttributes(&pa, src->p) == cudaSuccess && cudaPointerGetAttributes(&pb, dst->p) == cudaSuccess &&
+      pa.type == cudaMemoryTypeDevice && pb.type == cudaMemoryTypeDevice && pa.device == pb.device) {
+    pcg::AuxArgs a{};
+    a.state = view_of(src);
+    a.dst = view_of(dst);
+    for (int d = 0; d < 3; ++d) {
+      a.dlo[d] = lo[d];
+      a.dhi[d] = hi[d];
+    }
+    a.ncomp = src->ncomp;
+    const int64_t n = b.cells() * src->ncomp;
+    const cudaError_t e = pcg_strict::launch_aux(AUX_COPY, 1, a, (n + kThreads - 1) / kThreads, s);
+    return e == cudaSuccess ? PCG_OK : fail(PCG_ECUDA, "copy_cells: %s", cudaGetErrorString(e));
+  }
+  cudaGetLastError();
   // Whole rows in both arrays: each k-slice of the box is one contiguous run, so copy
   // slices rather than rows (host-to-device copies of short strided rows run at a
   // fraction of the bus bandwidth).
@@ -1261,6 +1297,10 @@ int pcg_plan_create(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* bo
   aux_segments(bx, P->aux_segs, P->aux_blocks);
   if (fuse) fuse_boxes(P->boxes);
   build_layout(P->L, P->boxes, prm);
+  if (P->L.oversize) {
+    delete P;
+    return fail(PCG_EINVAL, "a region needs workspace arrays of 2^31 elements or more: use smaller boxes or fuse = 0");
+  }
   cudaError_t e = cudaSuccess;
   if (P->L.ws_bytes) e = cudaMalloc(&P->ws, P->L.ws_bytes);
   if (e != cudaSuccess) {
@@ -1499,6 +1539,7 @@ extern "C" int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t 
   if ((rc = box_from_desc(b, pcg::nvar(prm->nspec), boxes[0]))) return rc;
   Layout L;
   build_layout(L, boxes, prm);
+  if (L.oversize) return fail(PCG_EINVAL, "box too large");
   // scratch = [tables | workspace]; the table size does not depend on the addresses
   Tables T;
   pack_tables(L, T);

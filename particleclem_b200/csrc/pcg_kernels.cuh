@@ -55,34 +55,37 @@ __device__ __forceinline__ double dt_of(const pcg::StageArgs& a, const pcg::Regi
   return a.dt_dev ? *a.dt_dev : rg.dt_ptr ? *rg.dt_ptr : rg.dt;
 }
 
+// Segment counts and block numbers stay below 2^31 (the host checks the launch sizes),
+// so the thread's position is formed with 32-bit (unsigned) division.
 __device__ __forceinline__ bool item_of(const pcg::StageArgs& a, Item& it) {
-  const int64_t blk = blockIdx.x;
+  const int blk = blockIdx.x;
   int lo = 0, hi = a.nseg - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (a.segs[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
   }
   const pcg::Seg& s = a.segs[lo];
-  const int64_t local = (blk - s.blk0) * blockDim.x + threadIdx.x;
-  if (local >= s.count) return false;
-  const int64_t t = local / s.n[0];
-  it.i = s.lo[0] + (int)(local - t * s.n[0]);
-  it.j = s.lo[1] + (int)(t % s.n[1]);
-  it.k = s.lo[2] + (int)(t / s.n[1]);
+  const unsigned local = unsigned(blk - (int)s.blk0) * blockDim.x + threadIdx.x;
+  if (local >= (unsigned)s.count) return false;
+  const unsigned n0 = s.n[0], n1 = s.n[1];
+  const unsigned t = local / n0;
+  it.i = s.lo[0] + (int)(local - t * n0);
+  it.j = s.lo[1] + (int)(t % n1);
+  it.k = s.lo[2] + (int)(t / n1);
   it.rg = a.regions + s.region;
   it.variant = s.variant;
   return true;
 }
 
 // The segment of this block and the block's index within it (tiled stages).
-__device__ __forceinline__ const pcg::Seg& seg_of(const pcg::StageArgs& a, int64_t& local_block) {
-  const int64_t blk = blockIdx.x;
+__device__ __forceinline__ const pcg::Seg& seg_of(const pcg::StageArgs& a, int& local_block) {
+  const int blk = blockIdx.x;
   int lo = 0, hi = a.nseg - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (a.segs[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
   }
-  local_block = blk - a.segs[lo].blk0;
+  local_block = blk - (int)a.segs[lo].blk0;
   return a.segs[lo];
 }
 
@@ -90,19 +93,19 @@ __device__ __forceinline__ const pcg::Seg& seg_of(const pcg::StageArgs& a, int64
 template <class T>
 struct CellPtr {
   T* p;
-  int64_t ns;
-  __device__ __forceinline__ T& operator[](int n) const { return p[(int64_t)n * ns]; }
+  int ns;
+  __device__ __forceinline__ T& operator[](int n) const { return p[n * ns]; }
 };
 template <class T>
 __device__ __forceinline__ CellPtr<T> at(const V4<T>& v, int i, int j, int k) {
   return CellPtr<T>{&v(i, j, k, 0), v.ns};
 }
 template <class T>
-__device__ __forceinline__ CellPtr<T> shift(const CellPtr<T>& c, int64_t off) {
+__device__ __forceinline__ CellPtr<T> shift(const CellPtr<T>& c, int off) {
   return CellPtr<T>{c.p + off, c.ns};
 }
 template <class T>
-__device__ __forceinline__ int64_t dstride(const V4<T>& v, int d) {
+__device__ __forceinline__ int dstride(const V4<T>& v, int d) {
   return d == 0 ? 1 : d == 1 ? v.js : v.ks;
 }
 
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
 template <class R> struct Prim;
 template <> struct Prim<double> {
   const double* p;
-  int64_t ns, st;
+  int ns, st;
   __device__ __forceinline__ Prim(const pcg::Region& rg, int i, int j, int k, int d) {
     const V4<const double> v = v4<const double>(rg.q);
     p = &v(i, j, k, 0);
@@ -330,7 +333,7 @@ template <> struct Prim<double> {
 };
 template <> struct Prim<float> {
   const float* p;
-  int64_t ns, st;
+  int ns, st;
   __device__ __forceinline__ Prim(const pcg::Region& rg, int i, int j, int k, int d) {
     const V4<const float> v = v4<const float>(rg.qf);
     p = &v(i, j, k, 0);
@@ -641,7 +644,7 @@ __device__ __forceinline__ void face_flux(const pcg::Region& rg, int i, int j, i
                                           R* fl, R& gun, R& gpres, R* qx = nullptr) {
   const V4<const double> qav = v4<const double>(rg.qa);
   const CellPtr<const double> qa = at(qav, i, j, k);
-  const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + (int64_t)pcg::QC * qa.ns]));
+  const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + pcg::QC * qa.ns]));
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
   cmpflx<NS, MIX, EXACT, D, R, QX>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav,
                                    R(p0_of<NS, MIX, R>(rg)), fl, gun, gpres, qx);
@@ -681,14 +684,15 @@ __global__ void __launch_bounds__(128, MINB) k_flux0(pcg::StageArgs a) {
 // The march of one thread of a y- or z-face stage (k_flux1, k_flux2): threads in linear
 // order over i (fastest), the row axis and the chunks of pcg::FACE_MARCH faces along D.
 template <int D>
-__device__ __forceinline__ bool march_of(const pcg::Seg& sg, int64_t t, int& i, int& r, int& m0, int& m1) {
+__device__ __forceinline__ bool march_of(const pcg::Seg& sg, int t, int& i, int& r, int& m0, int& m1) {
   constexpr int RA = (D == 1) ? 2 : 1;
-  const int64_t local = t * blockDim.x + threadIdx.x;
-  if (local >= pcg::face_threads(D, sg.n)) return false;
-  const int64_t q = local / sg.n[0];
-  i = sg.lo[0] + (int)(local - q * sg.n[0]);
-  r = sg.lo[RA] + (int)(q % sg.n[RA]);
-  m0 = sg.lo[D] + (int)(q / sg.n[RA]) * pcg::FACE_MARCH;
+  const unsigned local = unsigned(t) * blockDim.x + threadIdx.x;
+  if (local >= (unsigned)pcg::face_threads(D, sg.n)) return false;
+  const unsigned n0 = sg.n[0], nr = sg.n[RA];
+  const unsigned q = local / n0;
+  i = sg.lo[0] + (int)(local - q * n0);
+  r = sg.lo[RA] + (int)(q % nr);
+  m0 = sg.lo[D] + (int)(q / nr) * pcg::FACE_MARCH;
   m1 = min(m0 + pcg::FACE_MARCH, sg.lo[D] + sg.n[D]);
   return true;
 }
@@ -728,7 +732,7 @@ struct CorrArray {
 };
 
 template <int NS, class R>
-__device__ __forceinline__ void transdo_corr(const CellPtr<const R>& f, int64_t ostride, R cdtdx, R c, R p0, R* K) {
+__device__ __forceinline__ void transdo_corr(const CellPtr<const R>& f, int ostride, R cdtdx, R c, R p0, R* K) {
   const TransdoCorr<NS, R> kc{f, shift(f, ostride), cdtdx, c, p0};
   constexpr int NC = pcg::FL_Y + NS;
   if constexpr (sizeof(R) == 4) {
@@ -876,14 +880,15 @@ __device__ __forceinline__ void flux1_x_pair(const pcg::StageArgs& a, const pcg:
 }
 
 template <int NS, bool MIX, bool EXACT, class R>
-__device__ __forceinline__ void flux1_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kx) {
+__device__ __forceinline__ void flux1_x(const pcg::StageArgs& a, const pcg::Seg& sg, int t, R* kx) {
   const pcg::Region& rg = a.regions[sg.region];
-  const int64_t local = t * blockDim.x + threadIdx.x;
-  const bool active = local < sg.count;
-  const int64_t q = local / sg.n[0];
-  const int i = sg.lo[0] + (int)(local - q * sg.n[0]);
-  const int j = sg.lo[1] + (int)(q % sg.n[1]);
-  const int k = sg.lo[2] + (int)(q / sg.n[1]);
+  const unsigned local = unsigned(t) * blockDim.x + threadIdx.x;
+  const bool active = local < (unsigned)sg.count;
+  const unsigned n0 = sg.n[0], n1 = sg.n[1];
+  const unsigned q = local / n0;
+  const int i = sg.lo[0] + (int)(local - q * n0);
+  const int j = sg.lo[1] + (int)(q % n1);
+  const int k = sg.lo[2] + (int)(q / n1);
   const bool own_right = (threadIdx.x & 31) == 31 || i == sg.lo[0] + sg.n[0] - 1;
   const R p0 = R(p0_of<NS, MIX, R>(rg));
   flux1_x_pair<NS, MIX, EXACT, 1, R>(a, rg, active, own_right, i, j, k, p0, kx);
@@ -910,7 +915,7 @@ __device__ __forceinline__ void flux1_march_pair(const pcg::Region& rg, int i, i
 }
 
 template <int NS, bool MIX, bool EXACT, int D, class R>
-__device__ __forceinline__ void flux1_march(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kcarry) {
+__device__ __forceinline__ void flux1_march(const pcg::StageArgs& a, const pcg::Seg& sg, int t, R* kcarry) {
   const pcg::Region& rg = a.regions[sg.region];
   constexpr int RA = (D == 1) ? 2 : 1;  // row axis, also the second partner
   int i, r, m0, m1;
@@ -972,7 +977,7 @@ template <int NS, bool MIX, bool EXACT, class R, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux1(pcg::StageArgs a) {
   if constexpr (pcg::flux1_shared(sizeof(R))) {
     __shared__ R kcarry[2 * ncorr1<NS>() * 128];
-    int64_t t;
+    int t;
     const pcg::Seg& sg = seg_of(a, t);
     switch (sg.variant) {
       case 0: flux1_x<NS, MIX, EXACT, R>(a, sg, t, kcarry); break;
@@ -1005,8 +1010,8 @@ __global__ void __launch_bounds__(128, MINB) k_flux1(pcg::StageArgs a) {
 template <int NS> constexpr int ncorr() { return 7 + NS; }
 
 template <int NS, class R>
-__device__ __forceinline__ void transdd_corr(const CellPtr<const R>& fx, int64_t xst, const CellPtr<const R>& fy,
-                                             int64_t yst, R cdtdx0, R cdtdx1, R c, R p0, R* K) {
+__device__ __forceinline__ void transdd_corr(const CellPtr<const R>& fx, int xst, const CellPtr<const R>& fy,
+                                             int yst, R cdtdx0, R cdtdx1, R c, R p0, R* K) {
   const CellPtr<const R> gx = shift(fx, xst), gy = shift(fy, yst);
   constexpr int NC = pcg::FL_Y + NS;
   if constexpr (sizeof(R) == 4) {
@@ -1100,13 +1105,13 @@ __device__ __forceinline__ void transdd_apply(const R* qn, const R* K, R hdt, bo
 // fluxes of one d-face; T is the flux arithmetic type. The increments are formed as
 // visc * (u_i - u_{i-1}) in FP64, the reference's order of operations.
 template <int NS, int D, class T>
-__device__ __forceinline__ void adjust_fluxes(T* fl, const CellPtr<const double>& u, int64_t ud, double visc,
+__device__ __forceinline__ void adjust_fluxes(T* fl, const CellPtr<const double>& u, int ud, double visc,
                                               bool at_bndry) {
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); n++) {
     if (n == pcg::UTEMP) continue;
     const bool is_tang = (n == pcg::UMX || n == pcg::UMY || n == pcg::UMZ) && (n != pcg::UMX + D);
-    if (!(at_bndry && is_tang)) fl[n] += T(visc * (u[n] - u.p[-ud + (int64_t)n * u.ns]));
+    if (!(at_bndry && is_tang)) fl[n] += T(visc * (u[n] - u.p[-ud + n * u.ns]));
   }
   fl[pcg::UTEMP] = T(0);
   T summ = T(0);
@@ -1198,7 +1203,7 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   const double visc = rg.dx[D] * div;
   const V4<const double> uv = v4<const double>(rg.uin);
   const CellPtr<const double> u = at(uv, i, j, k);
-  const int64_t ud = dstride(uv, D);
+  const int ud = dstride(uv, D);
   const double ar = rg.area[D].p ? v4<const double>(rg.area[D])(i, j, k) : rg.area_u[D];
   if constexpr (PDev<R>::on) {
     if (rg.ff_single) {
@@ -1253,14 +1258,15 @@ __device__ __forceinline__ void flux2_consts(const pcg::StageArgs& a, const pcg:
 }
 
 template <int NS, bool MIX, bool EXACT, class R, bool UMETH = false>
-__device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kx) {
+__device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg& sg, int t, R* kx) {
   const pcg::Region& rg = a.regions[sg.region];
-  const int64_t local = t * blockDim.x + threadIdx.x;
-  const bool active = local < sg.count;
-  const int64_t q = local / sg.n[0];
-  const int i = sg.lo[0] + (int)(local - q * sg.n[0]);
-  const int j = sg.lo[1] + (int)(q % sg.n[1]);
-  const int k = sg.lo[2] + (int)(q / sg.n[1]);
+  const unsigned local = unsigned(t) * blockDim.x + threadIdx.x;
+  const bool active = local < (unsigned)sg.count;
+  const unsigned n0 = sg.n[0], n1 = sg.n[1];
+  const unsigned q = local / n0;
+  const int i = sg.lo[0] + (int)(local - q * n0);
+  const int j = sg.lo[1] + (int)(q % n1);
+  const int k = sg.lo[2] + (int)(q / n1);
   R cdtdx0, cdtdx1, hdt;
   double p0d;
   flux2_consts<NS, MIX, EXACT, R>(a, rg, 0, cdtdx0, cdtdx1, hdt, p0d);
@@ -1287,7 +1293,7 @@ __device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg&
 }
 
 template <int NS, bool MIX, bool EXACT, int D, class R, bool UMETH = false>
-__device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::Seg& sg, int64_t t, R* kcarry) {
+__device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::Seg& sg, int t, R* kcarry) {
   const pcg::Region& rg = a.regions[sg.region];
   int i, r, m0, m1;
   if (!march_of<D>(sg, t, i, r, m0, m1)) return;
@@ -1327,7 +1333,7 @@ __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::
 template <int NS, bool MIX, bool EXACT, class R, int MINB, bool UMETH = false>
 __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
   __shared__ R kcarry[2 * ncorr<NS>() * 128];
-  int64_t t;
+  int t;
   const pcg::Seg& sg = seg_of(a, t);
   switch (sg.variant) {
     case 0: flux2_x<NS, MIX, EXACT, R, UMETH>(a, sg, t, kcarry); break;

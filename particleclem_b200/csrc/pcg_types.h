@@ -42,6 +42,9 @@ constexpr int NEWTON_MAXIT = 20;
 constexpr double NEWTON_RTOL = 1.0e-10;
 constexpr double NEWTON_TMIN = 10.0;
 constexpr int MAXNS = 16;
+// The kernels address a view with 32-bit element offsets: every view the host passes them
+// (workspace arrays and the caller's arrays) spans fewer elements than this.
+constexpr int64_t kMaxViewElems = 2147483647;
 
 struct EosConst {
   int kind;  // 0 gamma law, 1 NASA-7 mixture
@@ -189,6 +192,7 @@ struct AuxArgs {
   const FillBox* fills; // batched ghost fill
   int32_t nfill;
   int32_t pad;
+  View dst;               // device box copy: destination (state is the source)
   const pcg::Seg* bsegs;  // per-box timestep: the advance segments of each region
   double* dt_boxes;       // per-box timestep result (device, one per region)
 };

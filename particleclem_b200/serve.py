@@ -120,21 +120,19 @@ class Scheduler:
                 progressed = True
             if waiting and len(inflight) < self.max_inflight:
                 batch, cells, rest = [], 0, []
-                stop = False
-                for r in waiting:
-                    if stop or r.pid in busy:
+                stop = len(waiting)  # index of the first request the scan did not reach
+                for idx, r in enumerate(waiting):
+                    if r.pid in busy:
                         rest.append(r)
                         continue
                     if batch and ((self.max_batch is not None and len(batch) >= self.max_batch) or (
                             self.max_batch_cells is not None and cells + r.cells > self.max_batch_cells)):
-                        stop = True
-                        rest.append(r)
-                        continue
+                        stop = idx
+                        break
                     need = r.nbytes + (0 if r.pid in self.resident else r.state_bytes)
                     if not self._evict_for(need, busy):
-                        stop = True  # first come first served: nothing overtakes a request that does not fit
-                        rest.append(r)
-                        continue
+                        stop = idx  # first come first served: nothing overtakes a request that does not fit
+                        break
                     if r.pid not in self.resident:
                         self.resident[r.pid] = r.state_bytes
                         self.uploads += 1
@@ -145,7 +143,7 @@ class Scheduler:
                     r.batch = self.nbatches
                     batch.append(r)
                     cells += r.cells
-                waiting = rest
+                waiting = rest + waiting[stop:]  # the passed-over requests keep their order
                 if batch:
                     self.peak_bytes = max(self.peak_bytes, self.used)
                     slots = {s for _, _, s in inflight}
@@ -345,8 +343,26 @@ def serve_sweep(executor, pids, budget_bytes, loads=(0.1, 0.25, 0.5, 0.75, 0.8, 
     ex = executor
     nreq = len(pids) if nreq is None else int(nreq)
     rng = np.random.default_rng(seed)
+    # the first saturated run warms the memory pool and the streams; the second is measured.
+    # The cyclic garbage collector is off while requests are served (its pauses would show
+    # as latency outliers of the host loop), and the interpreter switches threads every
+    # 0.2 ms so that a batch-completion watcher reaches the scheduler promptly.
+    import gc
+    import sys
+
+    gc_was, switch = gc.isenabled(), sys.getswitchinterval()
+    gc.disable()
+    sys.setswitchinterval(2e-4)
+    try:
+        return _sweep(ex, pids, budget_bytes, loads, nreq, rng, seed, max_inflight, max_batch_cells, out)
+    finally:
+        sys.setswitchinterval(switch)
+        if gc_was:
+            gc.enable()
+
+
+def _sweep(ex, pids, budget_bytes, loads, nreq, rng, seed, max_inflight, max_batch_cells, out):
     sat = None
-    # the first saturated run warms the memory pool and the streams; the second is measured
     for rep, load in enumerate((math.inf, math.inf) + tuple(loads)):
         arr = np.zeros(nreq) if load is math.inf else poisson_arrivals(nreq, load * sat, seed + rep)
         choice = rng.choice(np.asarray(pids), size=nreq)

@@ -22,6 +22,21 @@ point-to-point and all-reduce calls through torch.distributed (DistComm), or dir
 device copies between slabs held by one process (LocalComm, used to check the
 decomposition on one device). The global domain's physical boundaries (outflow in z for
 the flame) stay with the first and last slab; a periodic z wraps around the ranks.
+
+Overlapped form (``overlap=True``): the hydro advance of the slab's interior planes, whose
+4-cell stencil stays clear of the ghost planes the exchange fills, runs while the halo is
+in flight; only the NG-plane bands next to an exchanging slab face wait for it. A step is
+
+  1. local ghost fill and packing of the send planes (a device kernel)
+  2. the exchange posted (NCCL works on NCCL's stream, ordered after the packing)
+  3. hydro source of the interior region                 (runs during the exchange)
+  4. wait for the exchange; unpack (a device kernel); hydro source of the bands
+  5. S_new with computeTemp over the whole slab, then its CFL minimum
+  6. the minimum over ranks, which is the next step's timestep.
+
+Every region's hydro source is independent of how the level is cut (each output depends
+only on traced states of grow(region, 1), inside the grow(region, 4) stencil), so the
+overlapped step equals the plain one (bit for bit in the FP64 forms).
 """
 from __future__ import annotations
 
@@ -52,7 +67,8 @@ def halo_planes(state, ng=NG):
 class SlabStepper:
     """The device side of one rank's slab (see the module docstring)."""
 
-    def __init__(self, slab, nranks, rank, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, device=0, fused_tail=True):
+    def __init__(self, slab, nranks, rank, precision=abi.PREC_MIXED, fuse=True, cfl=0.3, device=0, fused_tail=True,
+                 overlap=False):
         import torch
 
         self.torch = torch
@@ -90,24 +106,60 @@ class SlabStepper:
         self.rbuf = {k: torch.zeros_like(v["recv_" + k]) for k in ("down", "up")}
         self.ncells = slab.ncells()
         self.graphs = None
+        # overlapped form: the interior region and the bands next to exchanging faces
+        self.plan_int = self.plan_bnd = None
+        int_z, bands = self.regions(slab.k0, slab.k1, self.down is not None, self.up is not None)
+        self.overlap = bool(overlap) and int_z is not None and bool(bands)
+        if self.overlap:
+            lo0, hi0 = (slab.domlo[0], slab.domlo[1]), (slab.domhi[0], slab.domhi[1])
+
+            def box(z):
+                return hydro.make_box((*lo0, z[0]), (*hi0, z[1]), self.state, self.hsrc, slab.dx, 0.0, slab.domlo,
+                                      slab.domhi, slab.bclo, slab.bchi)
+
+            self.plan_int = hydro.Plan(self.prm, [box(int_z)], fuse=True)
+            self.plan_bnd = hydro.Plan(self.prm, [box(b) for b in bands], fuse=False)
+
+    @staticmethod
+    def regions(k0, k1, has_down, has_up):
+        """z-ranges of the overlapped form: the interior (None if empty) and the bands of NG
+        planes next to the slab faces that receive ghost planes from a neighbour."""
+        lo = k0 + (NG if has_down else 0)
+        hi = k1 - (NG if has_up else 0)
+        bands = ([(k0, k0 + NG - 1)] if has_down else []) + ([(k1 - NG + 1, k1)] if has_up else [])
+        return ((lo, hi) if lo <= hi else None), bands
 
     # -- phases
     def fill(self):
         """Local part of the ghost fill (no exchange)."""
         hydro.fill_ghosts(self.state, self.fill_lo, self.fill_hi, self.fill_periodic, NG)
 
+    def _planes(self, z0, z1):
+        """The box of all x, y cells (ghosts included) of the planes z0..z1."""
+        sl = self.slab
+        return (sl.domlo[0] - NG, sl.domlo[1] - NG, z0), (sl.domhi[0] + NG, sl.domhi[1] + NG, z1)
+
     def fill_and_pack(self):
+        """Local ghost fill, then the NG lowest / highest valid planes into the send
+        buffers (one copy kernel each)."""
         self.fill()
+        k0, k1 = self.slab.k0, self.slab.k1
         if self.down is not None:
-            self.sbuf["down"].copy_(self.views["send_down"])
+            lo, hi = self._planes(k0, k0 + NG - 1)
+            hydro.copy_cells(self.state, abi.Fab(self.sbuf["down"], lo), lo, hi)
         if self.up is not None:
-            self.sbuf["up"].copy_(self.views["send_up"])
+            lo, hi = self._planes(k1 - NG + 1, k1)
+            hydro.copy_cells(self.state, abi.Fab(self.sbuf["up"], lo), lo, hi)
 
     def _unpack(self):
+        """The received planes into the ghost planes below / above the slab."""
+        k0, k1 = self.slab.k0, self.slab.k1
         if self.down is not None:
-            self.views["recv_down"].copy_(self.rbuf["down"])
+            lo, hi = self._planes(k0 - NG, k0 - 1)
+            hydro.copy_cells(abi.Fab(self.rbuf["down"], lo), self.state, lo, hi)
         if self.up is not None:
-            self.views["recv_up"].copy_(self.rbuf["up"])
+            lo, hi = self._planes(k1 + 1, k1 + NG)
+            hydro.copy_cells(abi.Fab(self.rbuf["up"], lo), self.state, lo, hi)
 
     def unpack_and_estdt(self):
         """Unpack the received ghost planes; the slab's CFL timestep into dt (its CFL
@@ -173,9 +225,29 @@ class SlabStepper:
         if i == 2 and self.fused_tail:
             self._primed = True
 
+    # -- overlapped form
+    def begin_step(self):
+        """The step's timestep: the previous step's minimum over ranks of the new state."""
+        self.dt.copy_(self.dt_next)
+
+    def hydro_interior(self):
+        self.plan_int.hydro(self.dt)
+
+    def unpack_and_hydro_bands(self):
+        self._unpack()
+        self.plan_bnd.hydro(self.dt)
+
+    def update_and_estdt(self):
+        """S_new with computeTemp over the slab, then its CFL minimum into dt_next."""
+        self.plan.update(self.dt)
+        self.plan.estdt(self.cfl, self.dt_next)
+
     def close(self):
         self.graphs = None
         self.plan.close()
+        for p in (self.plan_int, self.plan_bnd):
+            if p is not None:
+                p.close()
 
 
 class DistComm:
@@ -202,11 +274,34 @@ class DistComm:
             for r in dist.batch_isend_irecv(ops):
                 r.wait()
 
-    def min_dt(self, slabs):
+    def exchange_start(self, slabs):
+        """Post the exchange and return its works; with NCCL the transfer runs on NCCL's
+        stream after the work already queued (the packing), so later kernels overlap it."""
         import torch.distributed as dist
 
         (s,) = slabs
-        dist.all_reduce(s.dt, op=dist.ReduceOp.MIN)
+        ops = []
+        if s.down is not None:
+            ops.append(dist.P2POp(dist.isend, s.sbuf["down"], s.down))
+        if s.up is not None:
+            ops.append(dist.P2POp(dist.isend, s.sbuf["up"], s.up))
+        if s.up is not None:
+            ops.append(dist.P2POp(dist.irecv, s.rbuf["up"], s.up))
+        if s.down is not None:
+            ops.append(dist.P2POp(dist.irecv, s.rbuf["down"], s.down))
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    def exchange_wait(self, works, slabs):
+        """Order later work after the exchange (NCCL: the current stream waits; gloo: the
+        host waits)."""
+        for r in works:
+            r.wait()
+
+    def min_dt(self, slabs, attr="dt"):
+        import torch.distributed as dist
+
+        (s,) = slabs
+        dist.all_reduce(getattr(s, attr), op=dist.ReduceOp.MIN)
 
 
 class LocalComm:
@@ -219,12 +314,19 @@ class LocalComm:
                 u.rbuf["down"].copy_(s.sbuf["up"])
                 s.rbuf["up"].copy_(u.sbuf["down"])
 
-    def min_dt(self, slabs):
+    def exchange_start(self, slabs):
+        self.exchange(slabs)
+        return []
+
+    def exchange_wait(self, works, slabs):
+        pass
+
+    def min_dt(self, slabs, attr="dt"):
         import torch
 
-        m = torch.stack([s.dt for s in slabs]).min(dim=0).values
+        m = torch.stack([getattr(s, attr) for s in slabs]).min(dim=0).values
         for s in slabs:
-            s.dt.copy_(m)
+            getattr(s, attr).copy_(m)
 
 
 def step(slabs, comm):
@@ -238,3 +340,33 @@ def step(slabs, comm):
     comm.min_dt(slabs)
     for s in slabs:
         s.phase(2)
+
+
+def step_overlap(slabs, comm):
+    """One level step in the overlapped form (see the module docstring). The first step,
+    and a step after load_state, first take the fresh CFL timestep of the exchanged slabs.
+    Slabs too thin for an interior region (at most 2 NG planes between two exchanging
+    faces) take the plain step."""
+    if not all(s.overlap for s in slabs):
+        return step(slabs, comm)
+    for s in slabs:
+        s.fill_and_pack()
+    if not all(s._primed for s in slabs):
+        comm.exchange(slabs)
+        for s in slabs:
+            s._unpack()
+            s.plan.estdt(s.cfl, s.dt_next)
+        comm.min_dt(slabs, "dt_next")
+    for s in slabs:
+        s.begin_step()
+    works = comm.exchange_start(slabs)
+    for s in slabs:
+        s.hydro_interior()  # overlaps the halo exchange
+    comm.exchange_wait(works, slabs)
+    for s in slabs:
+        s.unpack_and_hydro_bands()
+    for s in slabs:
+        s.update_and_estdt()
+    comm.min_dt(slabs, "dt_next")
+    for s in slabs:
+        s._primed = True

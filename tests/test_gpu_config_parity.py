@@ -29,8 +29,12 @@ from particleclem_b200 import abi, hydro, workloads as wl
 
 pytestmark = pytest.mark.gpu
 
-# bound of the mixed form's hydro source (relative L1 per component, group-normalised)
-MIXED_SRC_TOL = 1e-4
+# Bound of the mixed form's hydro source (relative L1 per component, group-normalised).
+# Measured on B200: 1.5e-4 in rho E and rho e of the 32^3 flame box (the energy flux at
+# 1 atm is u (rho E + p), about 1e9 in CGS units, and its divergence across the box is a
+# small difference of such fluxes, each rounded to FP32), below 1e-5 elsewhere; the same
+# step's S_new is within 1.5e-8.
+MIXED_SRC_TOL = 5e-4
 
 
 @pytest.fixture(scope="module")

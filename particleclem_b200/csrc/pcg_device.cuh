@@ -77,6 +77,26 @@ __device__ __forceinline__ V4<T> v4(const pcg::View& w) {
   return V4<T>{reinterpret_cast<T*>(w.p), (int)w.js, (int)w.ks, (int)w.ns, w.b[0], w.b[1], w.b[2]};
 }
 
+// A view of a blocked workspace array (pcg::View::blocked, pcg::kCellBlock): cell(i, j, k)
+// is the address of component 0 of the cell; component n is kCellBlock * n elements on.
+template <class T>
+struct B4 {
+  T* p;
+  int js, ks, bs;
+  int bx, by, bz;
+  __device__ __forceinline__ T* cell(int i, int j, int k) const {
+    const int L = (i - bx) + (j - by) * js + (k - bz) * ks;
+    return p + ((L >> 5) * bs + (L & (pcg::kCellBlock - 1)));
+  }
+  __device__ __forceinline__ T& operator()(int i, int j, int k, int n = 0) const {
+    return cell(i, j, k)[n * pcg::kCellBlock];
+  }
+};
+template <class T>
+__device__ __forceinline__ B4<T> b4(const pcg::View& w) {
+  return B4<T>{reinterpret_cast<T*>(w.p), (int)w.js, (int)w.ks, (int)w.ns, w.b[0], w.b[1], w.b[2]};
+}
+
 // ------------------------------------------------------------------ EOS
 // PelePhysics' eos() restated (documented in the oracle): rmix = RU * sum Y_k / W_k;
 // gamma law: cs = sqrt(gamma P / R), e = P / ((gamma-1) R); NASA-7 mixture:

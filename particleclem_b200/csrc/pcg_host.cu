@@ -318,15 +318,20 @@ struct Layout {
   int64_t nblocks[K_NKIND] = {};
 };
 
-size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v) {
+// A workspace array of nc components over box b: Array4 layout, or with blocked != 0 the
+// blocked layout of pcg::View (cells in blocks of pcg::kCellBlock, all components of a
+// block together), which the arrays the flux stages pass on use.
+size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v, bool blocked = false) {
   const size_t off = (L.ws_bytes + kAlign - 1) / kAlign * kAlign;
   v.p = reinterpret_cast<void*>(off);  // rebased once the workspace exists
   v.js = b.n(0);
   v.ks = b.n(0) * b.n(1);
-  v.ns = b.cells();
+  const int64_t cells = blocked ? (b.cells() + pcg::kCellBlock - 1) / pcg::kCellBlock * pcg::kCellBlock : b.cells();
+  v.ns = blocked ? int64_t(pcg::kCellBlock) * nc : cells;
+  v.blocked = blocked ? 1 : 0;
   for (int d = 0; d < 3; ++d) v.b[d] = b.lo[d];
-  L.ws_bytes = off + size_t(b.cells()) * nc * esz;
-  if (b.cells() * nc > pcg::kMaxViewElems) L.oversize = true;
+  L.ws_bytes = off + size_t(cells) * nc * esz;
+  if (cells * nc > pcg::kMaxViewElems) L.oversize = true;
   return off;
 }
 
@@ -400,13 +405,13 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
     for (int d = 0; d < 3; ++d) {
       IBox tb = g1;
       tb.hi[d] += 1;  // d-faces lo-1 .. hi+2
-      take(L, tb, nt, L.esz, R.trm[d]);
-      take(L, tb, nt, L.esz, R.trp[d]);
+      take(L, tb, nt, L.esz, R.trm[d], true);
+      take(L, tb, nt, L.esz, R.trp[d], true);
       add_seg(L, K_TRACE, (int)r, d, g1);
     }
     for (int d = 0; d < 3; ++d) {
       IBox fb = nodes(grow_dir(g1, d, -1), d);  // d-faces lo..hi+1, others grown by 1
-      take(L, fb, nf, L.esz, R.fi[d]);
+      take(L, fb, nf, L.esz, R.fi[d], true);
       add_seg(L, K_FLUX0, (int)r, d, fb);
     }
     for (int d = 0; d < 3; ++d) {
@@ -415,7 +420,7 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
         const int t = 3 - d - o;
         IBox b = nodes(B.bx, d);
         b = grow_dir(b, t, 1);
-        take(L, b, nf, L.esz, R.fdo[d][o]);
+        take(L, b, nf, L.esz, R.fdo[d][o], true);
       }
       // one thread per d-face computes both (d|o) pairs that reach it
       add_seg(L, K_FLUX1, (int)r, d, nodes(grow_dir(g1, d, -1), d));
@@ -430,15 +435,17 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
     }
     for (int d = 0; d < 3; ++d) {
       const IBox fb = nodes(B.bx, d);
+      // the mixed form's FP32 final fluxes are workspace arrays in the blocked layout; FP64
+      // final fluxes (workspace or the caller's flux FABs) keep the Array4 layout
       if (B.flx[d].p) {
         R.ff[d] = B.flx[d];
       } else {
-        take(L, fb, nv, fsz, R.ff[d]);
+        take(L, fb, nv, fsz, R.ff[d], R.ff_single != 0);
       }
       if (B.umeth)
         R.qec[d] = B.qec[d];
       else
-        take(L, fb, 2, fsz, R.qec[d]);
+        take(L, fb, 2, fsz, R.qec[d], R.ff_single != 0);
       add_seg(L, K_FLUX2, (int)r, d, fb);
     }
     // Source/Godunov.cpp:440-468: faces of the box on an inflow or user_bc domain

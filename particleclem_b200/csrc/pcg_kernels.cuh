@@ -108,6 +108,21 @@ template <class T>
 __device__ __forceinline__ int dstride(const V4<T>& v, int d) {
   return d == 0 ? 1 : d == 1 ? v.js : v.ks;
 }
+// One cell of a blocked view: component n at p[n * kCellBlock] (a compile-time offset).
+template <class T>
+struct BCell {
+  T* p;
+  __device__ __forceinline__ T& operator[](int n) const { return p[n * pcg::kCellBlock]; }
+};
+template <class T>
+__device__ __forceinline__ BCell<T> at(const B4<T>& v, int i, int j, int k) {
+  return BCell<T>{v.cell(i, j, k)};
+}
+// the neighbour of (i, j, k) one cell up in direction d
+template <class T>
+__device__ __forceinline__ BCell<T> at_up(const B4<T>& v, int i, int j, int k, int d) {
+  return at(v, i + (d == 0), j + (d == 1), k + (d == 2));
+}
 
 // The pressure offset of a region for the FP32 arithmetic (see PDev): the ideal-gas
 // pressure RU * sum(rhoY_k / W_k) * T of the region's first valid cell, from the
@@ -422,8 +437,8 @@ __device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int 
     yp2[n] = Ip[2];
   }
 #undef PROFILE3
-  const CellPtr<R> qp = at(v4<R>(rg.trp[D]), i, j, k);
-  const CellPtr<R> qm = at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2));
+  const BCell<R> qp = at(b4<R>(rg.trp[D]), i, j, k);
+  const BCell<R> qm = at(b4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2));
   // plus state on face i (Source/PPM.cpp:232-331)
   {
     R rho_ref = Imr[0];
@@ -593,8 +608,8 @@ __device__ __forceinline__ void plm_cell(const pcg::Region& rg, int i, int j, in
 template <int NS, bool MIX, int D, class R>
 __device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
                                               double dt) {
-  plm_cell<NS, MIX, D, R>(rg, i, j, k, cc, flat, order, dt, at(v4<R>(rg.trp[D]), i, j, k),
-                          at(v4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2)));
+  plm_cell<NS, MIX, D, R>(rg, i, j, k, cc, flat, order, dt, at(b4<R>(rg.trp[D]), i, j, k),
+                          at(b4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2)));
 }
 
 template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R>
@@ -633,25 +648,27 @@ __global__ void __launch_bounds__(128) k_trace_weno(pcg::StageArgs a) {
 }
 
 // ------------------------------------------------------------------ flux stages
-template <int NS, class R>
-__device__ __forceinline__ void load_state(const CellPtr<R>& t, R* s) {
+template <int NS, class R, class C>
+__device__ __forceinline__ void load_state(const C& t, R* s) {
 #pragma unroll
   for (int n = 0; n < pcg::nt_comps(NS); ++n) s[n] = t[n];
 }
 
+// p0: the region's pressure offset of the FP32 arithmetic (p0_of), formed once by the
+// caller rather than per face (it reads the FP64 state of the region's first cell).
 template <int NS, bool MIX, bool EXACT, int D, class R, bool QX = false>
 __device__ __forceinline__ void face_flux(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr,
-                                          R* fl, R& gun, R& gpres, R* qx = nullptr) {
+                                          R p0, R* fl, R& gun, R& gpres, R* qx = nullptr) {
   const V4<const double> qav = v4<const double>(rg.qa);
   const CellPtr<const double> qa = at(qav, i, j, k);
   const R cav = R(0.5 * (qa[pcg::QC] + qa.p[-dstride(qav, D) + pcg::QC * qa.ns]));
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
-  cmpflx<NS, MIX, EXACT, D, R, QX>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav,
-                                   R(p0_of<NS, MIX, R>(rg)), fl, gun, gpres, qx);
+  cmpflx<NS, MIX, EXACT, D, R, QX>(ql, qr, idx, rg.bclo[D], rg.bchi[D], rg.domlo[D], rg.domhi[D], cav, p0, fl, gun,
+                                   gpres, qx);
 }
 
-template <int NS, class R>
-__device__ __forceinline__ void store_tflux(const CellPtr<R>& f, const R* fl, R gun, R gpres) {
+template <int NS, class R, class C>
+__device__ __forceinline__ void store_tflux(const C& f, const R* fl, R gun, R gpres) {
 #pragma unroll
   for (int n = 0; n < 5; ++n) f[n] = fl[n];
 #pragma unroll
@@ -664,10 +681,10 @@ __device__ __forceinline__ void store_tflux(const CellPtr<R>& f, const R* fl, R 
 template <int NS, bool MIX, bool EXACT, int D, class R>
 __device__ __forceinline__ void flux0_face(const pcg::Region& rg, int i, int j, int k) {
   R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)], fl[pcg::nvar(NS)], gun, gpres;
-  load_state<NS, R>(at(v4<R>(rg.trm[D]), i, j, k), ql);
-  load_state<NS, R>(at(v4<R>(rg.trp[D]), i, j, k), qr);
-  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, fl, gun, gpres);
-  store_tflux<NS, R>(at(v4<R>(rg.fi[D]), i, j, k), fl, gun, gpres);
+  load_state<NS, R>(at(b4<R>(rg.trm[D]), i, j, k), ql);
+  load_state<NS, R>(at(b4<R>(rg.trp[D]), i, j, k), qr);
+  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, R(p0_of<NS, MIX, R>(rg)), fl, gun, gpres);
+  store_tflux<NS, R>(at(b4<R>(rg.fi[D]), i, j, k), fl, gun, gpres);
 }
 
 template <int NS, bool MIX, bool EXACT, class R, int MINB>
@@ -706,9 +723,9 @@ __device__ __forceinline__ bool march_of(const pcg::Seg& sg, int t, int& i, int&
 template <int NS> constexpr int ncorr1() { return 6 + NS; }
 
 // The O-correction of one cell formed on demand from its two O-fluxes (component n of K).
-template <int NS, class R>
+template <int NS, class R, class C = BCell<const R>>
 struct TransdoCorr {
-  CellPtr<const R> f, g;
+  C f, g;  // the cell's first O-fluxes on its low and high O-faces
   R cdtdx, c, p0;
   __device__ __forceinline__ R operator()(int n) const {
     if (n < pcg::FL_Y + NS) return cdtdx * (g[n] - f[n]);
@@ -731,13 +748,12 @@ struct CorrArray {
   __device__ __forceinline__ R operator()(int n) const { return K[n]; }
 };
 
-template <int NS, class R>
-__device__ __forceinline__ void transdo_corr(const CellPtr<const R>& f, int ostride, R cdtdx, R c, R p0, R* K) {
-  const TransdoCorr<NS, R> kc{f, shift(f, ostride), cdtdx, c, p0};
+template <int NS, class R, class C>
+__device__ __forceinline__ void transdo_corr(const C& f, const C& g, R cdtdx, R c, R p0, R* K) {
+  const TransdoCorr<NS, R, C> kc{f, g, cdtdx, c, p0};
   constexpr int NC = pcg::FL_Y + NS;
   if constexpr (sizeof(R) == 4) {
     // the flux differences in component pairs with packed FP32 (FMUL2)
-    const CellPtr<const R> g = kc.g;
     const float2 c2 = make_float2(cdtdx, cdtdx);
 #pragma unroll
     for (int m = 0; m < NC / 2; ++m) {
@@ -802,9 +818,9 @@ __device__ __forceinline__ void transdo_apply(const R* qn, const KF& K, R p0, R*
 // its gamma_c.
 template <int NS, int O, class R>
 __device__ __forceinline__ void flux1_corr(const pcg::Region& rg, int i, int j, int k, R cdt, R p0, R* K) {
-  const V4<const R> fov = v4<const R>(rg.fi[O]);
+  const B4<const R> fov = b4<const R>(rg.fi[O]);
   const R c = R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC));
-  transdo_corr<NS, R>(at(fov, i, j, k), dstride(fov, O), cdt, c, p0, K);
+  transdo_corr<NS, R>(at(fov, i, j, k), at_up(fov, i, j, k, O), cdt, c, p0, K);
 }
 
 // The (D|O) flux at the D-face (i, j, k) from the left and right O-corrections
@@ -812,7 +828,7 @@ __device__ __forceinline__ void flux1_corr(const pcg::Region& rg, int i, int j, 
 template <int NS, bool EXACT, int D, int SIDE, class R, class KF>
 __device__ __forceinline__ void flux1_state_fn(const pcg::Region& rg, int i, int j, int k, const KF& K, R p0, R* q) {
   R qn[pcg::nt_comps(NS)];
-  load_state<NS, R>(at(v4<R>(SIDE == 0 ? rg.trm[D] : rg.trp[D]), i, j, k), qn);
+  load_state<NS, R>(at(b4<R>(SIDE == 0 ? rg.trm[D] : rg.trp[D]), i, j, k), qn);
   transdo_apply<NS, EXACT, R>(qn, K, p0, q);
 }
 template <int NS, bool EXACT, int D, int SIDE, class R>
@@ -823,16 +839,17 @@ __device__ __forceinline__ void flux1_state(const pcg::Region& rg, int i, int j,
 // The O-correction of the cell (i, j, k), formed on demand.
 template <int NS, int O, class R>
 __device__ __forceinline__ TransdoCorr<NS, R> flux1_corr_fn(const pcg::Region& rg, int i, int j, int k, R cdt, R p0) {
-  const V4<const R> fov = v4<const R>(rg.fi[O]);
-  const CellPtr<const R> f = at(fov, i, j, k);
-  return TransdoCorr<NS, R>{f, shift(f, dstride(fov, O)), cdt, R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC)), p0};
+  const B4<const R> fov = b4<const R>(rg.fi[O]);
+  return TransdoCorr<NS, R>{at(fov, i, j, k), at_up(fov, i, j, k, O), cdt,
+                            R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC)), p0};
 }
 
 template <int NS, bool MIX, bool EXACT, int D, int O, class R>
-__device__ __forceinline__ void flux1_riemann(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr) {
+__device__ __forceinline__ void flux1_riemann(const pcg::Region& rg, int i, int j, int k, const R* ql, const R* qr,
+                                              R p0) {
   R fl[pcg::nvar(NS)], gun, gpres;
-  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, fl, gun, gpres);
-  store_tflux<NS, R>(at(v4<R>(rg.fdo[D][O]), i, j, k), fl, gun, gpres);
+  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, p0, fl, gun, gpres);
+  store_tflux<NS, R>(at(b4<R>(rg.fdo[D][O]), i, j, k), fl, gun, gpres);
 }
 
 template <int NS, bool MIX, bool EXACT, int D, int O, class R>
@@ -841,7 +858,7 @@ __device__ __forceinline__ void flux1_solve(const pcg::Region& rg, int i, int j,
   R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
   flux1_state<NS, EXACT, D, 0, R>(rg, i, j, k, Kl, p0, ql);
   flux1_state<NS, EXACT, D, 1, R>(rg, i, j, k, Kr, p0, qr);
-  flux1_riemann<NS, MIX, EXACT, D, O, R>(rg, i, j, k, ql, qr);
+  flux1_riemann<NS, MIX, EXACT, D, O, R>(rg, i, j, k, ql, qr, p0);
 }
 
 template <int NS, class R>
@@ -911,7 +928,7 @@ __device__ __forceinline__ void flux1_march_pair(const pcg::Region& rg, int i, i
     K[n] = kl;
   }
   flux1_state<NS, EXACT, D, 0, R>(rg, i, j, k, K, p0, ql);
-  flux1_riemann<NS, MIX, EXACT, D, O, R>(rg, i, j, k, ql, qr);
+  flux1_riemann<NS, MIX, EXACT, D, O, R>(rg, i, j, k, ql, qr, p0);
 }
 
 template <int NS, bool MIX, bool EXACT, int D, class R>
@@ -961,7 +978,7 @@ __device__ __forceinline__ void flux1_face(const pcg::StageArgs& a, const pcg::R
     flux1_state_fn<NS, EXACT, D, 0, R>(rg, i, j, k, flux1_corr_fn<NS, O1, R>(rg, i - di, j - dj, k - dk, cdt, p0), p0,
                                     ql);
     flux1_state_fn<NS, EXACT, D, 1, R>(rg, i, j, k, flux1_corr_fn<NS, O1, R>(rg, i, j, k, cdt, p0), p0, qr);
-    flux1_riemann<NS, MIX, EXACT, D, O1, R>(rg, i, j, k, ql, qr);
+    flux1_riemann<NS, MIX, EXACT, D, O1, R>(rg, i, j, k, ql, qr, p0);
   }
   if (c[O2] >= rg.lo[O2] && c[O2] <= rg.hi[O2]) {
     const R cdt = flux1_cdt<NS, R>(a, rg, O2);
@@ -969,7 +986,7 @@ __device__ __forceinline__ void flux1_face(const pcg::StageArgs& a, const pcg::R
     flux1_state_fn<NS, EXACT, D, 0, R>(rg, i, j, k, flux1_corr_fn<NS, O2, R>(rg, i - di, j - dj, k - dk, cdt, p0), p0,
                                     ql);
     flux1_state_fn<NS, EXACT, D, 1, R>(rg, i, j, k, flux1_corr_fn<NS, O2, R>(rg, i, j, k, cdt, p0), p0, qr);
-    flux1_riemann<NS, MIX, EXACT, D, O2, R>(rg, i, j, k, ql, qr);
+    flux1_riemann<NS, MIX, EXACT, D, O2, R>(rg, i, j, k, ql, qr, p0);
   }
 }
 
@@ -1009,10 +1026,9 @@ __global__ void __launch_bounds__(128, MINB) k_flux1(pcg::StageArgs a) {
 // the reference's expressions in the reference's order.
 template <int NS> constexpr int ncorr() { return 7 + NS; }
 
-template <int NS, class R>
-__device__ __forceinline__ void transdd_corr(const CellPtr<const R>& fx, int xst, const CellPtr<const R>& fy,
-                                             int yst, R cdtdx0, R cdtdx1, R c, R p0, R* K) {
-  const CellPtr<const R> gx = shift(fx, xst), gy = shift(fy, yst);
+template <int NS, class R, class C>
+__device__ __forceinline__ void transdd_corr(const C& fx, const C& gx, const C& fy, const C& gy, R cdtdx0, R cdtdx1,
+                                             R c, R p0, R* K) {
   constexpr int NC = pcg::FL_Y + NS;
   if constexpr (sizeof(R) == 4) {
     // component pairs with packed FP32 (FFMA2)
@@ -1129,11 +1145,11 @@ __device__ __forceinline__ void flux2_corr(const pcg::Region& rg, int i, int j, 
                                            R* K) {
   constexpr int O1 = (D == 0) ? 1 : 0;
   constexpr int O2 = (D == 2) ? 1 : 2;
-  const V4<const R> fxv = v4<const R>(rg.fdo[O1][O2]);
-  const V4<const R> fyv = v4<const R>(rg.fdo[O2][O1]);
+  const B4<const R> fxv = b4<const R>(rg.fdo[O1][O2]);
+  const B4<const R> fyv = b4<const R>(rg.fdo[O2][O1]);
   const R c = R(v4<const double>(rg.qa)(i, j, k, pcg::QGAMC));
-  transdd_corr<NS, R>(at(fxv, i, j, k), dstride(fxv, O1), at(fyv, i, j, k), dstride(fyv, O2), cdtdx0, cdtdx1, c, p0,
-                      K);
+  transdd_corr<NS, R>(at(fxv, i, j, k), at_up(fxv, i, j, k, O1), at(fyv, i, j, k), at_up(fyv, i, j, k, O2), cdtdx0,
+                      cdtdx1, c, p0, K);
 }
 
 // One traced state of the D-face (i, j, k) after pc_transdd: SIDE 0 the left state
@@ -1146,7 +1162,7 @@ __device__ __forceinline__ void flux2_state(const pcg::Region& rg, int i, int j,
   CellPtr<const double> sq = has_src ? at(sqv, i, j, k) : CellPtr<const double>{nullptr, 0};
   if (SIDE == 0 && has_src) sq = shift(sq, -dstride(sqv, D));
   R qn[pcg::nt_comps(NS)];
-  load_state<NS, R>(at(v4<R>(SIDE == 0 ? rg.trm[D] : rg.trp[D]), i, j, k), qn);
+  load_state<NS, R>(at(b4<R>(SIDE == 0 ? rg.trm[D] : rg.trp[D]), i, j, k), qn);
   transdd_apply<NS, EXACT, R>(qn, K, hdt, has_src, sq, p0, q);
 }
 
@@ -1165,7 +1181,7 @@ __device__ __forceinline__ void umeth_face(const pcg::Region& rg, int i, int j, 
   constexpr int t1 = (D == 0) ? 1 : 0;
   constexpr int t2 = (D == 2) ? 1 : 2;
   R flr[pcg::nvar(NS)], gun, gpres, qx[3];
-  face_flux<NS, MIX, EXACT, D, R, true>(rg, i, j, k, ql, qr, flr, gun, gpres, qx);
+  face_flux<NS, MIX, EXACT, D, R, true>(rg, i, j, k, ql, qr, R(p0d), flr, gun, gpres, qx);
   const CellPtr<double> ff = at(v4<double>(rg.ff[D]), i, j, k);
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n)
@@ -1189,7 +1205,7 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
   constexpr int O1 = (D == 0) ? 1 : 0;
   constexpr int O2 = (D == 2) ? 1 : 2;
   R flr[pcg::nvar(NS)], gun, gpres;
-  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, flr, gun, gpres);
+  face_flux<NS, MIX, EXACT, D, R>(rg, i, j, k, ql, qr, R(p0d), flr, gun, gpres);
   // pc_artif_visc coefficient: difmag * min(0, average of the four nodal div u of the face)
   const V4<const double> dv = v4<const double>(rg.divu);
   const int ji = i + (O1 == 0), jj = j + (O1 == 1), jk = k + (O1 == 2);
@@ -1214,10 +1230,10 @@ __device__ __forceinline__ void flux2_face(const pcg::StageArgs& a, const pcg::R
       flr[pcg::UTEMP] = 0.f;
       adjust_fluxes<NS, D, float>(flr, u, ud, visc, at_bndry);
       const float arf = float(ar);
-      const CellPtr<float> ff = at(v4<float>(rg.ff[D]), i, j, k);
+      const BCell<float> ff = at(b4<float>(rg.ff[D]), i, j, k);
 #pragma unroll
       for (int n = 0; n < pcg::nvar(NS); ++n) ff[n] = flr[n] * arf;
-      const CellPtr<float> qe = at(v4<float>(rg.qec[D]), i, j, k);
+      const BCell<float> qe = at(b4<float>(rg.qec[D]), i, j, k);
       qe[0] = float(gpres);
       qe[1] = float(gun);
       return;
@@ -1433,14 +1449,36 @@ __global__ void __launch_bounds__(128) k_srctoprim(pcg::StageArgs a) {
 // accumulation. F is the element type of the final fluxes (double, or float with the
 // pressure as deviation from p0; p0 cancels in the flux differences and is added back to
 // the Godunov pressures of pdivu).
+// The final fluxes and face states of the cell's six faces: FP64 arrays (caller's or
+// workspace, Array4 layout) or the mixed form's FP32 workspace arrays (blocked layout).
+template <class F> struct FinalView;
+template <> struct FinalView<double> {
+  using C = CellPtr<const double>;
+  static __device__ __forceinline__ void cells(const pcg::View& w, int d, int i, int j, int k, C& lo, C& hi) {
+    const V4<const double> v = v4<const double>(w);
+    lo = at(v, i, j, k);
+    hi = shift(lo, dstride(v, d));
+  }
+};
+template <> struct FinalView<float> {
+  using C = BCell<const float>;
+  static __device__ __forceinline__ void cells(const pcg::View& w, int d, int i, int j, int k, C& lo, C& hi) {
+    const B4<const float> v = b4<const float>(w);
+    lo = at(v, i, j, k);
+    hi = at_up(v, i, j, k, d);
+  }
+};
+
 template <int NS, class F>
 __device__ __forceinline__ void consup_sum(const pcg::Region& rg, int i, int j, int k, double p0, double* h) {
-  const V4<const F> f0v = v4<const F>(rg.ff[0]), f1v = v4<const F>(rg.ff[1]), f2v = v4<const F>(rg.ff[2]);
-  const CellPtr<const F> f0 = at(f0v, i, j, k), f1 = at(f1v, i, j, k), f2 = at(f2v, i, j, k);
-  const CellPtr<const F> f0p = shift(f0, 1), f1p = shift(f1, f1v.js), f2p = shift(f2, f2v.ks);
-  const V4<const F> q0v = v4<const F>(rg.qec[0]), q1v = v4<const F>(rg.qec[1]), q2v = v4<const F>(rg.qec[2]);
-  const CellPtr<const F> q0 = at(q0v, i, j, k), q1 = at(q1v, i, j, k), q2 = at(q2v, i, j, k);
-  const CellPtr<const F> q0p = shift(q0, 1), q1p = shift(q1, q1v.js), q2p = shift(q2, q2v.ks);
+  using FV = FinalView<F>;
+  typename FV::C f0, f0p, f1, f1p, f2, f2p, q0, q0p, q1, q1p, q2, q2p;
+  FV::cells(rg.ff[0], 0, i, j, k, f0, f0p);
+  FV::cells(rg.ff[1], 1, i, j, k, f1, f1p);
+  FV::cells(rg.ff[2], 2, i, j, k, f2, f2p);
+  FV::cells(rg.qec[0], 0, i, j, k, q0, q0p);
+  FV::cells(rg.qec[1], 1, i, j, k, q1, q1p);
+  FV::cells(rg.qec[2], 2, i, j, k, q2, q2p);
   const bool ua = rg.area[0].p != nullptr;
   const V4<const double> a0 = v4<const double>(rg.area[0]);
   const V4<const double> a1 = v4<const double>(rg.area[1]);

@@ -69,11 +69,18 @@ struct EosConst {
 
 // A strided block of memory addressed like amrex::Array4 (element type decided by the
 // kernel that reads it): p[(i-b0) + (j-b1)*js + (k-b2)*ks + n*ns].
+// Blocked workspace arrays (the traced states and the face fluxes the flux stages pass
+// on) use the same linear cell index L = (i-b0) + (j-b1)*js + (k-b2)*ks but group the
+// cells in blocks of kCellBlock consecutive L, each block holding all its components one
+// after the other: element (L, n) at p[(L / 32) * ns + n * 32 + L % 32], ns = 32 * ncomp.
+// A warp reading one component of 32 consecutive cells still reads 128 contiguous bytes,
+// and the components of a cell are compile-time offsets from its first one.
+constexpr int kCellBlock = 32;
 struct View {
   void* p;
   int64_t js, ks, ns;
   int32_t b[3];
-  int32_t pad;
+  int32_t blocked;  // 1: blocked layout (ns is the block stride)
 };
 
 // Everything one box of a launch needs. Workspace views point into the library's

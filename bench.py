@@ -582,6 +582,7 @@ def run_ours(args):
             "precision_sweep": sweep,
             "gpu_launches": LevelStepper.launches_per_step * args.steps,  # fill 1, stages 6, fused tail 1, final dt 1
             "launch_variants": {f: {k: v["variant"] for k, v in t.items()} for f, t in tuned.items()},
+            "launch_tuning": tuned,
             "stage_ms": {n: float(v) for n, v in zip(names, stage_ms)},
             "roofline": roof,
             "path_roofline": path_roof,

@@ -283,7 +283,10 @@ int pcg_trim_workspace(int32_t device, int64_t keep_bytes);
 
 /* Each heavy stage (0 ctoprim, 2 trace, 3-5 Riemann stages) exists in three register
  * budgets (variants 0-2, increasingly tight); the library keeps the variant used
- * per (precision_mode, nspec, stage). particleclem_b200/autotune.py times them and
+ * per (precision_mode, nspec, stage). The trace of PCG_PREC_MIXED has variants 3-5 as
+ * well: the same budgets for the tiled trace, which stages each tile of the FP32
+ * primitive state and its halo in shared memory with one TMA load (plain PPM and PLM;
+ * the hybrid-WENO trace is never tiled). particleclem_b200/autotune.py times them and
  * sets the fastest. No counterpart in the reference (AMReX chooses launch shapes). */
 int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage, int32_t variant);
 /* Current variant, or a negative PCG_E* code. */

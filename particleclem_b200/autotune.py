@@ -3,7 +3,9 @@
 Every heavy stage (ctoprim, trace, the three Riemann stages, and the fused step tail
 that the consup slot selects for ``pcg_plan_advance``) is compiled in three register
 budgets (``kMinBlocks`` in csrc/pcg_kernels.cuh: no cap, moderate, tight),
-which trades registers per thread against resident warps per SM. The best choice
+which trades registers per thread against resident warps per SM; the trace of the
+mixed form also exists as the TMA-staged tiled trace in the same three budgets
+(variants 3-5). The best choice
 depends on the precision form (FP32 or FP64 arithmetic), the species count and the GPU,
 so it is measured: :func:`tune` runs each variant of each stage on a live plan with
 CUDA events, keeps the fastest, installs it with ``pcg_set_launch_variant`` and
@@ -20,6 +22,25 @@ TUNED_STAGES = (0, 2, 3, 4, 5)  # ctoprim, trace, flux0, flux1, flux2
 STAGE_NAMES = ("ctoprim", "prep", "trace", "flux0", "flux1", "flux2", "consup")
 TAIL_STAGE = 6  # the consup slot: its variant selects the fused step tail's register cap
 NVARIANT = 3
+TRACE_STAGE = 2
+TILED_TRACE_VARIANTS = 6  # the mixed form's trace: 0-2 untiled, 3-5 TMA-staged tiles
+
+
+def n_variants(prec, stage):
+    return TILED_TRACE_VARIANTS if (prec == 2 and stage == TRACE_STAGE) else NVARIANT
+
+
+CAPS = ("no register cap", "moderate register cap", "tight register cap")
+
+
+def describe(prec, stage, variant):
+    """What launch variant ``variant`` of ``stage`` is: its register budget, and for the
+    mixed form's trace whether it runs on TMA-staged tiles (32 x 4 cells per block for
+    the x and y traces, 32 x 1 x 4 for z) or one cell per thread from global memory."""
+    if stage == TRACE_STAGE and prec == 2:
+        shape = "TMA-staged tiles" if variant >= NVARIANT else "cell per thread"
+        return f"{shape}, {CAPS[variant % NVARIANT]}"
+    return CAPS[variant]
 
 
 def get_variant(prec, nspec, stage):
@@ -52,7 +73,8 @@ def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES, state=None):
         dt_next = torch.zeros(1, dtype=torch.float64, device=state.device)
     for st in stages:
         times = []
-        for v in range(NVARIANT):
+        nv = n_variants(prec, st)
+        for v in range(nv):
             set_variant(prec, ns, st, v)
             if st == TAIL_STAGE:
                 run = lambda: plan.advance(1.0, dt_dev, dt_next)  # noqa: E731
@@ -67,9 +89,10 @@ def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES, state=None):
             times.append(e0.elapsed_time(e1) / reps)
             if st == TAIL_STAGE:
                 state.copy_(saved)
-        best = min(range(NVARIANT), key=lambda v: times[v])
+        best = min(range(nv), key=lambda v: times[v])
         set_variant(prec, ns, st, best)
-        result[STAGE_NAMES[st]] = {"variant": best, "ms": [round(t, 4) for t in times]}
+        result[STAGE_NAMES[st]] = {"variant": best, "shape": describe(prec, st, best),
+                                   "ms": [round(t, 4) for t in times]}
     return result
 
 

@@ -524,23 +524,22 @@ __device__ __forceinline__ R vl_slope(R a, R b, R c) {
   return s;
 }
 
+// The interpolated value on the interface between a cell (value sl, van Leer slope dl)
+// and its right neighbour (sr, dr), bounded by the two cell values (Source/PPM.H:61-65
+// for sm, :93-97 for sp):
+// the edge sm of the right cell is the edge sp of the left one, so a caller that holds
+// the slopes of a row of cells forms each interface once.
 template <class R>
-__device__ __forceinline__ void ppm_reconstruct(const R s0, const R s1, const R s2, const R s3, const R s4,
-                                                const R flatn, R& sm, R& sp) {
-  {
-    const R dsvl_l = vl_slope(s0, s1, s2);
-    const R dsvl_r = vl_slope(s1, s2, s3);
-    sm = R(0.5) * (s2 + s1) - (R(1) / R(6)) * (dsvl_r - dsvl_l);
-    sm = dmax(sm, dmin(s2, s1));
-    sm = dmin(sm, dmax(s2, s1));
-  }
-  {
-    const R dsvl_l = vl_slope(s1, s2, s3);
-    const R dsvl_r = vl_slope(s2, s3, s4);
-    sp = R(0.5) * (s3 + s2) - (R(1) / R(6)) * (dsvl_r - dsvl_l);
-    sp = dmax(sp, dmin(s3, s2));
-    sp = dmin(sp, dmax(s3, s2));
-  }
+__device__ __forceinline__ R ppm_edge(const R sl, const R sr, const R dl, const R dr) {
+  R e = R(0.5) * (sr + sl) - (R(1) / R(6)) * (dr - dl);
+  e = dmax(e, dmin(sr, sl));
+  return dmin(e, dmax(sr, sl));
+}
+
+// Flattening and the monotonicity limiter of the parabola on the cell of value s2 with
+// interface values sm, sp (Source/PPM.H:99-114).
+template <class R>
+__device__ __forceinline__ void ppm_limit(const R s2, const R flatn, R& sm, R& sp) {
   sm = flatn * sm + (R(1) - flatn) * s2;
   sp = flatn * sp + (R(1) - flatn) * s2;
   if ((sp - s2) * (s2 - sm) <= R(0)) {
@@ -551,6 +550,15 @@ __device__ __forceinline__ void ppm_reconstruct(const R s0, const R s1, const R 
   } else if (fabs(sm - s2) >= R(2) * fabs(sp - s2)) {
     sm = R(3) * s2 - R(2) * sp;
   }
+}
+
+template <class R>
+__device__ __forceinline__ void ppm_reconstruct(const R s0, const R s1, const R s2, const R s3, const R s4,
+                                                const R flatn, R& sm, R& sp) {
+  const R d1 = vl_slope(s0, s1, s2), d2 = vl_slope(s1, s2, s3), d3 = vl_slope(s2, s3, s4);
+  sm = ppm_edge(s1, s2, d1, d2);
+  sp = ppm_edge(s2, s3, d2, d3);
+  ppm_limit(s2, flatn, sm, sp);
 }
 
 // Source/PPM.H:131-189 (ppm_int_profile), one wave

@@ -66,9 +66,26 @@ static cudaError_t launch_special(int stage, const pcg::StageArgs& a, const dim3
 }
 
 template <int NS, bool MIX, class R>
+static cudaError_t launch_trace_tile(const pcg::StageArgs& a, const dim3& grid, const dim3& block, int variant,
+                                    cudaStream_t s) {
+  if constexpr (sizeof(R) == 4) {
+    switch (variant) {
+      case 0: k_trace_tile<NS, MIX, kMinBlocks[K_TRACE][0]><<<grid, block, 0, s>>>(a); break;
+      case 1: k_trace_tile<NS, MIX, kMinBlocks[K_TRACE][1]><<<grid, block, 0, s>>>(a); break;
+      case 2: k_trace_tile<NS, MIX, kMinBlocks[K_TRACE][2]><<<grid, block, 0, s>>>(a); break;
+      default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  } else {
+    return cudaErrorInvalidValue;  // the FP64 forms trace from the global array
+  }
+}
+
+template <int NS, bool MIX, class R>
 static cudaError_t launch_t(int stage, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
   if (nblocks <= 0) return cudaSuccess;
   const dim3 grid((unsigned)nblocks), block(128);
+  if (stage == K_TRACE_TILE) return launch_trace_tile<NS, MIX, R>(a, grid, block, variant, s);
   if (stage == K_SRCQ || (a.umeth && (stage == K_FLUX2 || stage == K_LOWBC || stage == K_CONSUP)))
     return launch_special<NS, MIX, R>(stage, a, grid, block, s);
   switch (variant) {

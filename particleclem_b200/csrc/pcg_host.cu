@@ -19,6 +19,9 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "../../include/pcg_hydro.h"
 #include "pcg_types.h"
 
@@ -90,8 +93,9 @@ namespace {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
 // launches that are not stages of their own: the low-order inflow/user_bc faces, run as
-// part of stage K_FLUX2 right after it, and pc_srctoprim (pcg_srctoprim)
-enum { K_LOWBC = K_NSTAGE, K_SRCQ, K_NKIND };
+// part of stage K_FLUX2 right after it, pc_srctoprim (pcg_srctoprim), and the TMA-staged
+// trace that stands in for stage K_TRACE in the mixed form
+enum { K_LOWBC = K_NSTAGE, K_SRCQ, K_TRACE_TILE, K_NKIND };
 enum { AUX_ESTDT = 0, AUX_ESTDT_FINAL, AUX_UPDATE, AUX_FILL, AUX_FILL_BOXES, AUX_ESTDT_BOXES, AUX_COPY };
 constexpr int kThreads = 128;
 constexpr size_t kAlign = 256;
@@ -100,13 +104,17 @@ thread_local std::string g_err;
 
 // Launch-variant table: [precision_mode][species slot][stage] -> variant index of
 // kMinBlocks (pcg_kernels.cuh). Defaults measured on B200 for the production flame
-// level; pcg_set_launch_variant (the autotuner) overrides them.
+// level; pcg_set_launch_variant (the autotuner) overrides them. The mixed form's trace
+// has three more variants: 3-5 run the TMA-staged tiled trace (K_TRACE_TILE) with the
+// register budgets 0-2.
+constexpr int kTileVariant = 3;
 std::mutex g_var_mu;
 int g_variant[3][2][7] = {
   {{0, 0, 2, 0, 2, 2, 2}, {2, 0, 1, 1, 2, 0, 2}},  // FP64 reference order
   {{2, 0, 1, 0, 0, 0, 2}, {2, 0, 1, 0, 0, 0, 2}},  // FP64 with FMA
   {{0, 0, 2, 0, 2, 0, 2}, {2, 0, 2, 2, 2, 1, 2}},  // mixed
 };
+int max_variant(int prec, int stage) { return (prec == PCG_PREC_MIXED && stage == K_TRACE) ? 5 : 2; }
 int variant_of(int prec, int ns, int stage) {
   std::lock_guard<std::mutex> lk(g_var_mu);
   return g_variant[prec][ns == 1 ? 0 : 1][stage];
@@ -309,6 +317,7 @@ struct BoxIn {
 
 struct Layout {
   bool oversize = false;  // a workspace array would span 2^31 elements or more
+  bool tile_trace = false;  // the mixed form's trace runs as TMA-staged tiles (K_TRACE_TILE)
   int ns = 1;
   int umeth = 0;  // the plan is a pcg_umeth call
   size_t esz = 8;  // compute-type size of the intermediates
@@ -321,12 +330,15 @@ struct Layout {
 // A workspace array of nc components over box b: Array4 layout, or with blocked != 0 the
 // blocked layout of pcg::View (cells in blocks of pcg::kCellBlock, all components of a
 // block together), which the arrays the flux stages pass on use.
-size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v, bool blocked = false) {
+// With pad_rows the rows of an Array4-layout array are padded to a multiple of 4 elements
+// (16 bytes for FP32), as the TMA tensor maps of the staged trace need.
+size_t take(Layout& L, const IBox& b, int nc, size_t esz, pcg::View& v, bool blocked = false, bool pad_rows = false) {
   const size_t off = (L.ws_bytes + kAlign - 1) / kAlign * kAlign;
   v.p = reinterpret_cast<void*>(off);  // rebased once the workspace exists
-  v.js = b.n(0);
-  v.ks = b.n(0) * b.n(1);
-  const int64_t cells = blocked ? (b.cells() + pcg::kCellBlock - 1) / pcg::kCellBlock * pcg::kCellBlock : b.cells();
+  v.js = pad_rows ? (b.n(0) + 3) / 4 * 4 : b.n(0);
+  v.ks = v.js * b.n(1);
+  const int64_t cells = blocked ? (b.cells() + pcg::kCellBlock - 1) / pcg::kCellBlock * pcg::kCellBlock
+                                : v.ks * b.n(2);
   v.ns = blocked ? int64_t(pcg::kCellBlock) * nc : cells;
   v.blocked = blocked ? 1 : 0;
   for (int d = 0; d < 3; ++d) v.b[d] = b.lo[d];
@@ -347,6 +359,40 @@ void add_seg(Layout& L, int stage, int region, int variant, const IBox& b) {
   L.nblocks[stage] += tiled ? pcg::face_tiles(variant, s.n) : (s.count + kThreads - 1) / kThreads;
 }
 
+// The tiled trace of direction d over g1 = grow(box,1), as K_TRACE_TILE segments: the up
+// to three disjoint strips that full tiles cannot cover, along x, y and z (variant d:
+// one cell per thread, read from global memory), and the full tiles of the rest
+// (variant 3 + d).
+void add_trace_tiles(Layout& L, int region, int d, const IBox& g1) {
+  const int tn[3] = {pcg::kTraceTileX, pcg::trace_tile_y(d), pcg::trace_tile_z(d)};
+  int64_t core[3];
+  for (int e = 0; e < 3; ++e) core[e] = g1.n(e) / tn[e] * tn[e];
+  const bool tiles = core[0] > 0 && core[1] > 0 && core[2] > 0;
+  if (!tiles) core[0] = 0;  // no tile: the x strip is all of g1
+  // strip e: cells past the core along e, inside the core along the directions before e
+  for (int e = 0; e < 3; ++e) {
+    IBox b = g1;
+    b.lo[e] = g1.lo[e] + (int)core[e];
+    for (int f = 0; f < e; ++f) b.hi[f] = g1.lo[f] + (int)core[f] - 1;
+    bool empty = false;
+    for (int f = 0; f < 3; ++f) empty = empty || b.n(f) <= 0;
+    if (!empty) add_seg(L, K_TRACE_TILE, region, d, b);
+    if (!tiles) break;
+  }
+  if (!tiles) return;
+  pcg::Seg sg{};
+  sg.region = region;
+  sg.variant = 3 + d;
+  for (int e = 0; e < 3; ++e) {
+    sg.lo[e] = g1.lo[e];
+    sg.n[e] = (int)(core[e] / tn[e]);
+  }
+  sg.count = int64_t(sg.n[0]) * sg.n[1] * sg.n[2];
+  sg.blk0 = L.nblocks[K_TRACE_TILE];
+  L.segs[K_TRACE_TILE].push_back(sg);
+  L.nblocks[K_TRACE_TILE] += sg.count;
+}
+
 void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_params* prm) {
   const int ns = prm->nspec;
   const bool single = prm->precision_mode == PCG_PREC_MIXED;
@@ -354,6 +400,9 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
   const int qf_grow = (prm->use_hybrid_weno && prm->ppm_type == 1 && prm->weno_scheme == 2) ? 4 : 3;
   L.ns = ns;
   L.esz = single ? 4 : 8;
+  // the mixed form traces from TMA-staged shared-memory tiles of its FP32 primitive copy
+  // (PPM without hybrid WENO, and PLM)
+  L.tile_trace = single && !prm->use_hybrid_weno;
   const int nt = pcg::nt_comps(ns), nf = pcg::nf_comps(ns), nv = pcg::nvar(ns), nq = pcg::qvar(ns);
   for (size_t r = 0; r < boxes.size(); ++r) {
     const BoxIn& B = boxes[r];
@@ -395,7 +444,7 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
       // prep's flattening reads +-3 cells around grow(box,1) from this copy when ctoprim
       // wrote it, so it covers grow(box,4) then
       R.qf_grow = B.internal_q ? 4 : qf_grow;
-      take(L, grow(B.bx, R.qf_grow), nt, 4, R.qf);
+      take(L, grow(B.bx, R.qf_grow), nt, 4, R.qf, false, true);
       R.qf_in_prep = B.internal_q ? 0 : 1;
       add_seg(L, K_PREP, (int)r, 0, B.internal_q ? g1 : grow(B.bx, qf_grow));
     } else {
@@ -408,6 +457,7 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
       take(L, tb, nt, L.esz, R.trm[d], true);
       take(L, tb, nt, L.esz, R.trp[d], true);
       add_seg(L, K_TRACE, (int)r, d, g1);
+      if (L.tile_trace) add_trace_tiles(L, (int)r, d, g1);
     }
     for (int d = 0; d < 3; ++d) {
       IBox fb = nodes(grow_dir(g1, d, -1), d);  // d-faces lo..hi+1, others grown by 1
@@ -502,10 +552,54 @@ struct Tables {
   size_t bytes = 0;
   const pcg::Region* regions = nullptr;
   const pcg::Seg* segs[K_NKIND] = {};
+  const void* tmaps = nullptr;  // tensor maps of the TMA-staged trace (3 per region)
+  int32_t* err = nullptr;       // device error word
+  bool maps_ok = false;         // every tensor map encoded
   std::vector<char> host;
 };
 
-void pack_tables(const Layout& L, Tables& T) {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// The three tensor maps of a region's FP32 primitive copy qf (x fastest, then y, z,
+// component), with the boxes of the x, y and z traces (pcg::trace_box_*): 40 x 4 x 1,
+// 36 x 8 x 1 and 36 x 1 x 8 cells, every component.
+bool encode_trace_maps(const pcg::Region& R, int nc, char* out) {
+  PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+  if (!enc || !R.qf.p) return false;
+  const uintptr_t base = reinterpret_cast<uintptr_t>(R.qf.p);
+  if (base % 16 || R.qf.js % 4 || R.qf.blocked) return false;
+  const cuuint64_t dims[4] = {cuuint64_t(R.qf.js), cuuint64_t(R.qf.ks / R.qf.js), cuuint64_t(R.qf.ns / R.qf.ks),
+                              cuuint64_t(nc)};
+  const cuuint64_t strides[3] = {cuuint64_t(R.qf.js) * 4, cuuint64_t(R.qf.ks) * 4, cuuint64_t(R.qf.ns) * 4};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  for (int d = 0; d < 3; ++d) {
+    const cuuint32_t box[4] = {cuuint32_t(pcg::trace_box_x(d)), cuuint32_t(pcg::trace_box_y(d)),
+                               cuuint32_t(pcg::trace_box_z(d)), cuuint32_t(nc)};
+    CUtensorMap* m = reinterpret_cast<CUtensorMap*>(out + d * pcg::kTensorMapBytes);
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, reinterpret_cast<void*>(base), dims, strides,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+  }
+  return true;
+}
+
+// encode = false: sizing only, before the workspace addresses exist (no tensor maps).
+void pack_tables(const Layout& L, Tables& T, bool encode = true) {
+  static_assert(sizeof(CUtensorMap) == pcg::kTensorMapBytes, "CUtensorMap size");
   size_t off = L.regions.size() * sizeof(pcg::Region);
   size_t seg_off[K_NKIND];
   for (int s = 0; s < K_NKIND; ++s) {
@@ -513,29 +607,45 @@ void pack_tables(const Layout& L, Tables& T) {
     seg_off[s] = off;
     off += L.segs[s].size() * sizeof(pcg::Seg);
   }
-  T.bytes = std::max<size_t>(off, 16);
+  off = (off + 127) / 128 * 128;  // tensor maps: 64-byte aligned (the table base is 256-aligned)
+  const size_t map_off = off;
+  if (L.tile_trace) off += L.regions.size() * 3 * pcg::kTensorMapBytes;
+  const size_t err_off = off;
+  off += 16;
+  T.bytes = off;
   T.host.assign(T.bytes, 0);
   if (!L.regions.empty()) std::memcpy(T.host.data(), L.regions.data(), L.regions.size() * sizeof(pcg::Region));
   for (int s = 0; s < K_NKIND; ++s)
     if (!L.segs[s].empty()) std::memcpy(T.host.data() + seg_off[s], L.segs[s].data(), L.segs[s].size() * sizeof(pcg::Seg));
+  T.maps_ok = L.tile_trace && encode;
+  for (size_t r = 0; r < L.regions.size() && T.maps_ok; ++r)
+    T.maps_ok = encode_trace_maps(L.regions[r], pcg::nt_comps(L.ns),
+                                  T.host.data() + map_off + r * 3 * pcg::kTensorMapBytes);
   // device pointers are filled in by bind_tables once T.dev exists
   for (int s = 0; s < K_NKIND; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(seg_off[s]);
+  T.tmaps = reinterpret_cast<const void*>(map_off);
+  T.err = reinterpret_cast<int32_t*>(err_off);
 }
 
 void bind_tables(Tables& T) {
   char* base = static_cast<char*>(T.dev);
   T.regions = reinterpret_cast<const pcg::Region*>(base);
+  T.tmaps = base + reinterpret_cast<size_t>(T.tmaps);
+  T.err = reinterpret_cast<int32_t*>(base + reinterpret_cast<size_t>(T.err));
   for (int s = 0; s < K_NKIND; ++s) T.segs[s] = reinterpret_cast<const pcg::Seg*>(base + reinterpret_cast<size_t>(T.segs[s]));
 }
 
-int launch_kind(const Layout& L, const Tables& T, const pcg_hydro_params* p, int kind, const double* dt_dev,
-                cudaStream_t s) {
-  if (L.nblocks[kind] == 0) return PCG_OK;
+// One launch of the kernel of `stage` over the segments of kind `segs` (launch variant var).
+int launch_segs(const Layout& L, const Tables& T, const pcg_hydro_params* p, int stage, int segs, int var,
+                const double* dt_dev, cudaStream_t s) {
+  if (L.nblocks[segs] == 0) return PCG_OK;
   const bool single = p->precision_mode == PCG_PREC_MIXED;
   pcg::StageArgs a{};
+  a.tmaps = T.tmaps;
+  a.err = T.err;
   a.regions = T.regions;
-  a.segs = T.segs[kind];
-  a.nseg = (int32_t)L.segs[kind].size();
+  a.segs = T.segs[segs];
+  a.nseg = (int32_t)L.segs[segs].size();
   a.ppm_type = p->ppm_type;
   a.plm_iorder = p->plm_iorder;
   a.use_flattening = p->use_flattening;
@@ -544,12 +654,22 @@ int launch_kind(const Layout& L, const Tables& T, const pcg_hydro_params* p, int
   a.umeth = L.umeth;
   a.difmag = p->difmag;
   a.dt_dev = dt_dev;
-  const int var = kind < K_NSTAGE ? variant_of(p->precision_mode, L.ns, kind) : 0;
   cudaError_t e = (p->precision_mode == PCG_PREC_FP64)
-                    ? pcg_strict::launch_stage(kind, L.ns, false, a, L.nblocks[kind], var, s)
-                    : pcg_fast::launch_stage(kind, L.ns, single, a, L.nblocks[kind], var, s);
-  if (e != cudaSuccess) return fail(PCG_ECUDA, "stage %d launch: %s", kind, cudaGetErrorString(e));
+                    ? pcg_strict::launch_stage(stage, L.ns, false, a, L.nblocks[segs], var, s)
+                    : pcg_fast::launch_stage(stage, L.ns, single, a, L.nblocks[segs], var, s);
+  if (e != cudaSuccess) return fail(PCG_ECUDA, "stage %d launch: %s", stage, cudaGetErrorString(e));
   return PCG_OK;
+}
+
+int launch_kind(const Layout& L, const Tables& T, const pcg_hydro_params* p, int kind, const double* dt_dev,
+                cudaStream_t s) {
+  int var = kind < K_NSTAGE ? variant_of(p->precision_mode, L.ns, kind) : 0;
+  if (var >= kTileVariant) {
+    var -= kTileVariant;
+    // the mixed form's tiled trace (variants 3-5), when every tensor map was encoded
+    if (kind == K_TRACE && L.tile_trace && T.maps_ok) kind = K_TRACE_TILE;
+  }
+  return launch_segs(L, T, p, kind, kind, var, dt_dev, s);
 }
 
 int launch_stages(const Layout& L, const Tables& T, const pcg_hydro_params* p, int first, int last,
@@ -1017,7 +1137,7 @@ int pcg_step_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* box
   }
   // one stream-ordered allocation: [workspace | tables | fill table | block minima]
   Tables T;
-  pack_tables(L, T);
+  pack_tables(L, T, false);
   const size_t off_t = (L.ws_bytes + kAlign - 1) / kAlign * kAlign;
   const size_t off_f = off_t + (T.bytes + kAlign - 1) / kAlign * kAlign;
   const size_t off_p = off_f + (fills.size() * sizeof(pcg::FillBox) + kAlign - 1) / kAlign * kAlign;
@@ -1090,7 +1210,7 @@ int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t
   build_layout(L, bs, prm);
   if (L.oversize) return fail(PCG_EINVAL, "a region needs workspace arrays of 2^31 elements or more: use smaller boxes");
   Tables T;
-  pack_tables(L, T);
+  pack_tables(L, T, false);
   *bytes = int64_t((L.ws_bytes + kAlign - 1) / kAlign * kAlign + T.bytes);
   return PCG_OK;
 }
@@ -1439,7 +1559,7 @@ int pcg_trim_workspace(int32_t device, int64_t keep_bytes) {
 
 int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage, int32_t variant) {
   if (precision_mode < 0 || precision_mode > 2 || (nspec != 1 && nspec != 9) || stage < 0 || stage >= K_NSTAGE ||
-      variant < 0 || variant > 2)
+      variant < 0 || variant > max_variant(precision_mode, stage))
     return fail(PCG_EINVAL, "launch variant (%d, %d, %d, %d) out of range", precision_mode, nspec, stage, variant);
   std::lock_guard<std::mutex> lk(g_var_mu);
   g_variant[precision_mode][nspec == 1 ? 0 : 1][stage] = variant;
@@ -1549,7 +1669,7 @@ extern "C" int pcg_hydro_box_noalloc(const pcg_hydro_params* prm, const int32_t 
   if (L.oversize) return fail(PCG_EINVAL, "box too large");
   // scratch = [tables | workspace]; the table size does not depend on the addresses
   Tables T;
-  pack_tables(L, T);
+  pack_tables(L, T, false);
   const size_t ws_off = (T.bytes + kAlign - 1) / kAlign * kAlign;
   const size_t need = ws_off + L.ws_bytes;
   if (need > kNoAllocScratchBytes)

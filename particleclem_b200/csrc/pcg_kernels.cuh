@@ -22,13 +22,15 @@
 #pragma once
 
 #include "pcg_device.cuh"
+#include "pcg_tma.cuh"
 
 namespace PCG_TU {
 
 enum { K_CTOPRIM = 0, K_PREP, K_TRACE, K_FLUX0, K_FLUX1, K_FLUX2, K_CONSUP, K_NSTAGE };
 // launches that are not stages of their own: the inflow/user_bc boundary faces (within
-// stage K_FLUX2) and pc_srctoprim (pcg_srctoprim)
-enum { K_LOWBC = K_NSTAGE, K_SRCQ };
+// stage K_FLUX2), pc_srctoprim (pcg_srctoprim) and the TMA-staged trace (stage K_TRACE of
+// the mixed form)
+enum { K_LOWBC = K_NSTAGE, K_SRCQ, K_TRACE_TILE };
 
 // Launch variants: each heavy stage is compiled with a few minimum-resident-blocks
 // requests (__launch_bounds__ register caps); the host picks one per (form, species
@@ -329,6 +331,7 @@ __global__ void __launch_bounds__(128) k_prep(pcg::StageArgs a) {
 // pressure as the deviation from the box's p0), so no conversions are left in the trace.
 template <class R> struct Prim;
 template <> struct Prim<double> {
+  static constexpr bool kEdges = false;  // no precomputed PPM interface values
   const double* p;
   int ns, st;
   __device__ __forceinline__ Prim(const pcg::Region& rg, int i, int j, int k, int d) {
@@ -347,6 +350,7 @@ template <> struct Prim<double> {
   }
 };
 template <> struct Prim<float> {
+  static constexpr bool kEdges = false;
   const float* p;
   int ns, st;
   __device__ __forceinline__ Prim(const pcg::Region& rg, int i, int j, int k, int d) {
@@ -369,8 +373,16 @@ template <> struct Prim<float> {
 // trace: the PPM parabola (Source/PPM.H:28-115), or with HYB the hybrid-WENO edge values
 // of Source/PPM.cpp:120-172 (weno_scheme 0 WENO-JS5, 1 WENO-Z5, 2 WENO-Z7, 3 WENO-Z3,
 // any other value the PPM parabola).
-template <bool HYB, class R>
-__device__ __forceinline__ void ppm_edges(const Prim<R>& P, int qcomp, R flat, int scheme, R& sm, R& sp, R& sc) {
+template <bool HYB, class R, class PT>
+__device__ __forceinline__ void ppm_edges(const PT& P, int qcomp, R flat, int scheme, R& sm, R& sp, R& sc) {
+  if constexpr (PT::kEdges && !HYB) {
+    // the accessor holds the interface values of the parabola (ppm_edge), formed once
+    // per interface: only flattening and the limiter remain per cell
+    P.edges(qcomp, sm, sp);
+    sc = P.c(qcomp);
+    ppm_limit<R>(sc, flat, sm, sp);
+    return;
+  }
   if constexpr (HYB) {
     if (scheme == 2) {
       R s7[7];
@@ -399,12 +411,13 @@ __device__ __forceinline__ void ppm_edges(const Prim<R>& P, int qcomp, R flat, i
 // Source/PPM.cpp:82-423 for one cell and direction D (bx == vbx as called from
 // Source/Godunov.cpp:188-200, so both states are produced). Only the components the
 // path reads are reconstructed: QGAME, QREINT and QTEMP profiles feed nothing.
-template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R>
-__device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, double dt,
-                                              int scheme) {
+// P: the primitive state around the cell (Prim: the global array; PrimTile: a staged
+// shared-memory tile), with c(q), five(q, s) and stencil<W>(q, s) along D.
+template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R, class PT>
+__device__ __forceinline__ void trace_ppm_dir(const pcg::Region& rg, const PT& P, int i, int j, int k, R cc, R flat,
+                                              double dt, int scheme) {
   using E = Eos<NS, MIX, R>;
   using ER = EosR<NS, MIX, R>;
-  const Prim<R> P(rg, i, j, k, D);
   const R dtdx = R(dt / rg.dx[D]);
   const R un = P.c(pcg::QU + D);
   R sm, sp, sc, s6;
@@ -519,12 +532,11 @@ struct RegState {
 // Source/PLM.H:167-309 (pc_plm_d) with the slopes of Source/Godunov.cpp:139-180, for the
 // cell (i, j, k) and direction D: qp receives the state on the cell's low D-face (the
 // right state of that face), qm the state on its high D-face (the left state there).
-template <int NS, bool MIX, int D, class R, class QP, class QM>
-__device__ __forceinline__ void plm_cell(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
-                                         double dt, const QP& qp, const QM& qm) {
+template <int NS, bool MIX, int D, class R, class QP, class QM, class PT>
+__device__ __forceinline__ void plm_cell_p(const pcg::Region& rg, const PT& P, R cc, R flat, int order, double dt,
+                                           const QP& qp, const QM& qm) {
   constexpr int l1 = (D == 0) ? 1 : 0;
   constexpr int l2 = (D == 2) ? 1 : 2;
-  const Prim<R> P(rg, i, j, k, D);
   R s[5];
   const R p0 = R(p0_of<NS, MIX, R>(rg));
 #define SLOPE(comp) (P.five(comp, s), plm_slope<R>(s[0], s[1], s[2], s[3], s[4], flat, order))
@@ -605,22 +617,28 @@ __device__ __forceinline__ void plm_cell(const pcg::Region& rg, int i, int j, in
 #undef SLOPE
 }
 
-template <int NS, bool MIX, int D, class R>
-__device__ __forceinline__ void trace_plm_dir(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
-                                              double dt) {
-  plm_cell<NS, MIX, D, R>(rg, i, j, k, cc, flat, order, dt, at(b4<R>(rg.trp[D]), i, j, k),
-                          at(b4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2)));
+template <int NS, bool MIX, int D, class R, class QP, class QM>
+__device__ __forceinline__ void plm_cell(const pcg::Region& rg, int i, int j, int k, R cc, R flat, int order,
+                                         double dt, const QP& qp, const QM& qm) {
+  plm_cell_p<NS, MIX, D, R>(rg, Prim<R>(rg, i, j, k, D), cc, flat, order, dt, qp, qm);
 }
 
-template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R>
-__device__ __forceinline__ void trace_cell(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R, class PT>
+__device__ __forceinline__ void trace_cell_p(const pcg::StageArgs& a, const pcg::Region& rg, const PT& P, int i, int j,
+                                             int k) {
   const CellPtr<const R> pr = at(v4<const R>(rg.prep), i, j, k);
   const R flat = pr[0], cc = pr[1];
   const double dt = dt_of(a, rg);
   if (a.ppm_type == 1)
-    trace_ppm_dir<NS, MIX, EXACT, HYB, D, R>(rg, i, j, k, cc, flat, dt, a.weno_scheme);
+    trace_ppm_dir<NS, MIX, EXACT, HYB, D, R>(rg, P, i, j, k, cc, flat, dt, a.weno_scheme);
   else
-    trace_plm_dir<NS, MIX, D, R>(rg, i, j, k, cc, flat, a.plm_iorder, dt);
+    plm_cell_p<NS, MIX, D, R>(rg, P, cc, flat, a.plm_iorder, dt, at(b4<R>(rg.trp[D]), i, j, k),
+                              at(b4<R>(rg.trm[D]), i + (D == 0), j + (D == 1), k + (D == 2)));
+}
+
+template <int NS, bool MIX, bool EXACT, bool HYB, int D, class R>
+__device__ __forceinline__ void trace_cell(const pcg::StageArgs& a, const pcg::Region& rg, int i, int j, int k) {
+  trace_cell_p<NS, MIX, EXACT, HYB, D, R>(a, rg, Prim<R>(rg, i, j, k, D), i, j, k);
 }
 
 template <int NS, bool MIX, bool EXACT, class R, int MINB>
@@ -631,6 +649,197 @@ __global__ void __launch_bounds__(128, MINB) k_trace(pcg::StageArgs a) {
     case 0: trace_cell<NS, MIX, EXACT, false, 0, R>(a, *it.rg, it.i, it.j, it.k); break;
     case 1: trace_cell<NS, MIX, EXACT, false, 1, R>(a, *it.rg, it.i, it.j, it.k); break;
     default: trace_cell<NS, MIX, EXACT, false, 2, R>(a, *it.rg, it.i, it.j, it.k); break;
+  }
+}
+
+// ------------------------------------------------------------------ TMA-staged trace
+// The trace of the mixed form on full tiles of 128 cells (pcg::trace_tile_y/z), one cell
+// per thread. One TMA load stages the FP32 primitive copy of the tile and its two-cell
+// halo along the traced direction D (every component) in shared memory; every stencil of
+// the trace then reads the tile at compile-time offsets from the cell. The tiles cover
+// the largest part of grow(box,1) that they fill exactly, so no lane of a tile idles; the
+// same launch traces the strips left over (narrower than a tile) one cell per thread
+// from global memory (segment variants 0-2 strips, 3-5 tiles, of direction variant % 3).
+// The PPM interface values of a tile (ppm_tile_edges): for each reconstructed component
+// (the trace-state components but rho e, slot e_slot), along D the interfaces of every
+// row of the tile, the low face of each cell and one past the last.
+template <int D>
+struct TileEdges {
+  static constexpr int ROW = D == 0 ? pcg::kTraceTileX + 1 : pcg::kTraceTileX;  // x: 33 faces per row
+  static constexpr int NROW = D == 0 ? 4 : 5;  // y, z: 5 face rows of 32
+  static constexpr int PLANE = ROW * NROW;
+  static constexpr int ST = D == 0 ? 1 : pcg::kTraceTileX;  // from a cell's low face to its high face
+  // van Leer slopes of the cells of the tile and one more on each side along D
+  static constexpr int DROW = D == 0 ? pcg::kTraceTileX + 2 : pcg::kTraceTileX;
+  static constexpr int DPLANE = D == 0 ? DROW * 4 : DROW * 6;
+};
+__host__ __device__ constexpr int edge_slot(int tr) { return tr < pcg::TR_RE ? tr : tr - 1; }
+__host__ __device__ constexpr int slot_tr(int e) { return e < pcg::TR_RE ? e : e + 1; }
+
+template <int D>
+struct PrimTile {
+  static constexpr bool kEdges = true;
+  static constexpr int BX = pcg::trace_box_x(D), BY = pcg::trace_box_y(D);
+  static constexpr int PLANE = pcg::trace_box_cells(D);
+  static constexpr int ST = D == 0 ? 1 : D == 1 ? BX : BX * BY;
+  const float* p;  // component 0 of the cell in the tile
+  const float* e;  // interface values: slot 0 on the cell's low face
+  __device__ __forceinline__ float c(int qcomp) const { return p[tr_comp(qcomp) * PLANE]; }
+  __device__ __forceinline__ void edges(int qcomp, float& sm, float& sp) const {
+    const float* b = e + edge_slot(tr_comp(qcomp)) * TileEdges<D>::PLANE;
+    sm = b[0];
+    sp = b[TileEdges<D>::ST];
+  }
+  __device__ __forceinline__ void five(int qcomp, float* s) const { stencil<2>(qcomp, s); }
+  template <int W>
+  __device__ __forceinline__ void stencil(int qcomp, float* s) const {
+    const float* b = p + tr_comp(qcomp) * PLANE;
+#pragma unroll
+    for (int o = -W; o <= W; ++o) s[o + W] = b[o * ST];
+  }
+};
+
+// The PPM interface values of every reconstructed component of the staged tile along D,
+// each formed once (the per-cell form evaluates three van Leer slopes and two interfaces
+// per cell and component): the slopes of the tile's cells and of one more cell on each
+// side along D, then the interfaces. ox: the x offset of the tile's first cell in the
+// staged box. For x the four warps work on their own rows; for y and z the rows along D
+// belong to different warps, so the block synchronises between the phases.
+template <int NS, int D>
+__device__ __forceinline__ void ppm_tile_edges(const float* tile, int ox, float* dsv, float* edg) {
+  using P = PrimTile<D>;
+  using G = TileEdges<D>;
+  constexpr int NE = pcg::nt_comps(NS) - 1;
+  const int lane = int(threadIdx.x) % 32, w = int(threadIdx.x) / 32;
+  if constexpr (D == 0) {
+    // row w; slope index m: cell x0 - 1 + m (m < 34); interface index f: low face of x0 + f
+    const float* row = tile + w * P::BX + ox - 1;  // the cell x0 - 1
+    float* drow = dsv + w * G::DROW;
+    float* erow = edg + w * G::ROW;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+      const float* q = row + slot_tr(e) * P::PLANE + lane;
+      drow[e * G::DPLANE + lane] = vl_slope<float>(q[-1], q[0], q[1]);
+    }
+    if (lane < 2 * NE) {  // slopes 32 and 33 of every component
+      const int e = lane >> 1, m = 32 + (lane & 1);
+      const float* q = row + slot_tr(e) * P::PLANE + m;
+      drow[e * G::DPLANE + m] = vl_slope<float>(q[-1], q[0], q[1]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+      const float* q = row + slot_tr(e) * P::PLANE + lane;  // cells x0-1+lane (left), x0+lane
+      const float* d = drow + e * G::DPLANE + lane;
+      erow[e * G::PLANE + lane] = ppm_edge<float>(q[0], q[1], d[0], d[1]);
+    }
+    if (lane < NE) {  // face 32 of every component
+      const float* q = row + slot_tr(lane) * P::PLANE + 32;
+      const float* d = drow + lane * G::DPLANE + 32;
+      erow[lane * G::PLANE + 32] = ppm_edge<float>(q[0], q[1], d[0], d[1]);
+    }
+    __syncwarp();
+  } else {
+    // slope row m: cells D0 - 1 + m (m < 6), staged row m + 1; face row f: low face of
+    // D0 + f (f < 5), between staged rows f + 1 and f + 2 (D0 the tile's first y or z)
+    constexpr int RS = P::ST;  // staged-row stride along D
+    const float* col = tile + ox + lane;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int m = w + 4 * h;
+      if (h == 0 || m < 6) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+          const float* q = col + slot_tr(e) * P::PLANE + (m + 1) * RS;
+          dsv[e * G::DPLANE + m * 32 + lane] = vl_slope<float>(q[-RS], q[0], q[RS]);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int f = w + 4 * h;
+      if (h == 0 || f < 5) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+          const float* q = col + slot_tr(e) * P::PLANE + (f + 1) * RS;
+          const float* d = dsv + e * G::DPLANE + f * 32 + lane;
+          edg[e * G::PLANE + f * 32 + lane] = ppm_edge<float>(q[0], q[RS], d[0], d[32]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int NS, bool MIX, int D>
+__device__ __forceinline__ void trace_tile(const pcg::StageArgs& a, const pcg::Seg& sg, int t, float* tile,
+                                           float* dsv, float* edg, uint64_t* bar) {
+  using P = PrimTile<D>;
+  constexpr int NC = pcg::nt_comps(NS), TY = pcg::trace_tile_y(D), TZ = pcg::trace_tile_z(D);
+  const pcg::Region& rg = a.regions[sg.region];
+  const int ntx = sg.n[0], nty = sg.n[1];
+  const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+  const int x0 = sg.lo[0] + pcg::kTraceTileX * tx, y0 = sg.lo[1] + TY * ty, z0 = sg.lo[2] + TZ * tz;
+  const int qx = rg.qf.b[0], qy = rg.qf.b[1], qz = rg.qf.b[2];
+  int xs = (D == 0) ? x0 - 2 : x0;
+  xs -= (xs - qx) & 3;  // a multiple of 4 elements from the array's first x
+  const int ys = (D == 1) ? y0 - 2 : y0, zs = (D == 2) ? z0 - 2 : z0;
+  if (threadIdx.x == 0) {
+    const void* tmap = static_cast<const char*>(a.tmaps) + (size_t(sg.region) * 3 + D) * pcg::kTensorMapBytes;
+    mbar_arrive_expect_tx(bar, P::PLANE * NC * 4);
+    tma_load_4d(tile, tmap, xs - qx, ys - qy, zs - qz, 0, bar);
+  }
+  // every thread waits for the load; if any gave up, the whole block leaves (after a second
+  // bounded wait, as the load may still land), so that the block's barriers stay uniform
+  const bool landed = mbar_wait_bounded(bar, 0);
+  if (__syncthreads_or(!landed)) {
+    if (threadIdx.x == 0 && a.err) atomicOr(a.err, 1);
+    if (!landed) mbar_wait_bounded(bar, 0);
+    return;
+  }
+  if (a.ppm_type == 1) ppm_tile_edges<NS, D>(tile, x0 - xs, dsv, edg);
+  const int lane = int(threadIdx.x) % pcg::kTraceTileX, row = int(threadIdx.x) / pcg::kTraceTileX;
+  const int i = x0 + lane, j = y0 + (TY > 1 ? row : 0), k = z0 + (TZ > 1 ? row : 0);
+  if (i > rg.hi[0] + 1 || j > rg.hi[1] + 1 || k > rg.hi[2] + 1) return;  // tiles lie in grow(box, 1)
+  const P prim{tile + ((k - zs) * P::BY + (j - ys)) * P::BX + (i - xs), edg + row * TileEdges<D>::ROW + lane};
+  trace_cell_p<NS, MIX, false, false, D, float>(a, rg, prim, i, j, k);
+}
+
+template <int NS, bool MIX, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_trace_tile(pcg::StageArgs a) {
+  constexpr int kBoxMax = pcg::trace_box_cells(1) > pcg::trace_box_cells(2) ? pcg::trace_box_cells(1)
+                                                                             : pcg::trace_box_cells(2);
+  static_assert(pcg::trace_box_cells(0) <= kBoxMax, "tile buffer");
+  constexpr int NE = pcg::nt_comps(NS) - 1;
+  constexpr int kDsv = TileEdges<1>::DPLANE > TileEdges<0>::DPLANE ? TileEdges<1>::DPLANE : TileEdges<0>::DPLANE;
+  constexpr int kEdg = TileEdges<1>::PLANE > TileEdges<0>::PLANE ? TileEdges<1>::PLANE : TileEdges<0>::PLANE;
+  __shared__ __align__(128) float tile[kBoxMax * pcg::nt_comps(NS)];
+  __shared__ float dsv[NE * kDsv];  // van Leer slopes (PPM)
+  __shared__ float edg[NE * kEdg];  // interface values (PPM)
+  __shared__ __align__(8) uint64_t bar;
+  int t;
+  const pcg::Seg& sg = seg_of(a, t);
+  if (sg.variant < 3) {  // a strip: one cell per thread (the block's segment is uniform)
+    const unsigned local = unsigned(t) * blockDim.x + threadIdx.x;
+    if (local >= (unsigned)sg.count) return;
+    const unsigned n0 = sg.n[0], n1 = sg.n[1];
+    const unsigned r = local / n0;
+    const int i = sg.lo[0] + (int)(local - r * n0), j = sg.lo[1] + (int)(r % n1), k = sg.lo[2] + (int)(r / n1);
+    const pcg::Region& rg = a.regions[sg.region];
+    switch (sg.variant) {
+      case 0: trace_cell<NS, MIX, false, false, 0, float>(a, rg, i, j, k); break;
+      case 1: trace_cell<NS, MIX, false, false, 1, float>(a, rg, i, j, k); break;
+      default: trace_cell<NS, MIX, false, false, 2, float>(a, rg, i, j, k); break;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  switch (sg.variant) {
+    case 3: trace_tile<NS, MIX, 0>(a, sg, t, tile, dsv, edg, &bar); break;
+    case 4: trace_tile<NS, MIX, 1>(a, sg, t, tile, dsv, edg, &bar); break;
+    default: trace_tile<NS, MIX, 2>(a, sg, t, tile, dsv, edg, &bar); break;
   }
 }
 

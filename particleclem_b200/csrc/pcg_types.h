@@ -162,7 +162,23 @@ struct StageArgs {
   double difmag;
   const double* dt_dev;  // nullptr: each region's dt
   double* partial;       // fused step tail: one timestep minimum per block
+  const void* tmaps;     // TMA-staged trace: 3 tensor maps (x, y, z boxes) per region
+  int32_t* err;          // device error word: bit 0 set when a bounded TMA wait gave up
 };
+// The tiles of the TMA-staged trace, one per block of 128 threads: 32 cells along x by 4
+// along y (x and y traces) or along z (z trace), so that the 4 warps of a block are the
+// tile's 4 rows and the traced direction's neighbours are lanes (x) or warps (y, z). The
+// staged box adds the +-2 cells of the stencil along the traced direction, and along x up
+// to 3 more cells, because a box starts at a 16-byte boundary of the array.
+constexpr int kTraceTileX = 32;
+PCG_HD constexpr int trace_tile_y(int d) { return d == 2 ? 1 : 4; }
+PCG_HD constexpr int trace_tile_z(int d) { return d == 2 ? 4 : 1; }
+PCG_HD constexpr int trace_box_x(int d) { return d == 0 ? 40 : 36; }
+PCG_HD constexpr int trace_box_y(int d) { return d == 0 ? 4 : d == 1 ? 8 : 1; }
+PCG_HD constexpr int trace_box_z(int d) { return d == 2 ? 8 : 1; }
+PCG_HD constexpr int trace_box_cells(int d) { return trace_box_x(d) * trace_box_y(d) * trace_box_z(d); }
+// Bytes of one CUtensorMap (the layout of the driver's opaque type).
+constexpr int kTensorMapBytes = 128;
 
 // One box for the auxiliary kernels (timestep, state update).
 struct AuxBox {

@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline work budget")
     ap.add_argument("--serve-requests", type=int, default=5000, help="step requests per serving load point")
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0])
-    ap.add_argument("--serve-batch-cells", type=int, default=2_000_000, help="cells per serving batch at most")
+    ap.add_argument("--serve-batch-cells", type=int, default=500_000, help="cells per serving batch at most")
+    ap.add_argument("--serve-inflight", type=int, default=3, help="serving batches running at once (streams)")
     ap.add_argument("--sweep-steps", type=int, default=100, help="steps of the precision sweep")
     ap.add_argument("--no-side-workloads", action="store_true",
                     help="skip the batching, precision-sweep and serving workloads (quick runs)")
@@ -511,14 +512,16 @@ def run_ours(args):
 
     # ---- serving: patch-step latency under Poisson arrivals with continuous batching
     # (16 ensemble runs x 32 flame patches of edges in {16..64}; every request one step of
-    # a resident, evolving patch; HBM budget 120 GB; two streams)
+    # a resident, evolving patch; HBM budget 120 GB; batches of at most --serve-batch-cells
+    # cells, --serve-inflight of them at once on their own streams)
     from particleclem_b200.serve import ensemble_serving
 
     serving = None
     if not args.no_side_workloads:
         serving = ensemble_serving(lev.eos, nruns=16, per_run=32, seed=5 + rank, nreq=args.serve_requests,
                                    budget_bytes=int(120e9), loads=tuple(args.serve_loads),
-                                   max_batch_cells=args.serve_batch_cells, error_sample=32, device=local)
+                                   max_batch_cells=args.serve_batch_cells, error_sample=32, device=local,
+                                   max_inflight=args.serve_inflight)
 
     # ---- batching (512 independent flame boxes, edges log-uniform in [8, 64]) and the
     # precision sweep (256^3 periodic turbulence as 64 boxes of 64^3, PPM and PLM): mixed
@@ -569,7 +572,8 @@ def run_ours(args):
                     "serial": {"value": e2e_serial, "ms_per_step": mse_serial / ke,
                                "path": "same copies and step, one after another"}},
             "serving": None if serving is None else {"workload": serving["workload"], "budget_gb": serving["budget_gb"],
-                        "max_batch_cells": serving["max_batch_cells"],
+                        "max_batch_cells": serving["max_batch_cells"], "max_inflight": args.serve_inflight,
+                        "latency": "arrival to the host's observation of the batch's device completion",
                         "resident_state_gb": serving["resident_state_gb"],
                         "saturated_cell_updates_per_s": serving["points"][0]["cell_updates_per_s"],
                         "saturated_requests_per_s": serving["points"][0]["requests_per_s"],

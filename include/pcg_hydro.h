@@ -278,6 +278,12 @@ int pcg_plan_destroy(pcg_plan* plan);
  * returns all but keep_bytes of the pool of CUDA device `device` to the driver (after
  * the work that used it completes). No counterpart in the reference. */
 int pcg_trim_workspace(int32_t device, int64_t keep_bytes);
+/* Grows that pool to hold at least `bytes` (one allocation and its release; returns when
+ * done): a loop of one-shot calls whose workspace sizes vary (a serving loop) then takes
+ * its workspace from memory the pool holds, where the first call of each new size would
+ * otherwise wait for the driver to map memory (tens to hundreds of milliseconds
+ * measured on B200). No counterpart in the reference. */
+int pcg_reserve_workspace(int32_t device, int64_t bytes);
 
 /* ---- launch tuning ------------------------------------------------------------- */
 

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <deque>
 #include <vector>
 
 #include <cuda.h>
@@ -152,11 +153,77 @@ cudaError_t workspace_pool(cudaMemPool_t* pool) {
   return cudaSuccess;
 }
 
+// Allocation sizes are rounded up to size classes (from 1 MiB on, 4 to 7 units of a power
+// of two, at most 25 % over): the one-shot calls of a serving loop ask for a different
+// workspace size nearly every time, and without classes the pool keeps mapping new
+// memory for sizes that no freed block fits (tens of milliseconds per call, measured),
+// while a freed block of a class serves every later request of that class.
+size_t size_class(size_t bytes) {
+  if (bytes <= (size_t(1) << 20)) return bytes;
+  int k = 63 - __builtin_clzll(bytes);  // 2^k <= bytes < 2^(k+1)
+  const size_t unit = size_t(1) << (k - 2);
+  return (bytes + unit - 1) / unit * unit;
+}
+
 cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t s) {
   cudaMemPool_t pool = nullptr;
   cudaError_t e = workspace_pool(&pool);
   if (e != cudaSuccess) return e;
-  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+  return cudaMallocFromPoolAsync(p, size_class(bytes), pool, s);
+}
+
+// Pinned staging buffers for the table uploads of one-shot calls. A copy from pageable
+// host memory goes through the driver's few staging buffers, so once a handful of calls
+// are queued on a busy stream the next one blocks until the device has drained the
+// earlier copies: the host then waits for the device call after call. Here each upload
+// takes a pinned buffer that no queued copy still reads (an event recorded after its
+// last copy has completed), or a new one; buffers are kept for the life of the process.
+struct Staging {
+  void* host = nullptr;
+  size_t bytes = 0;
+  int device = -1;
+  cudaEvent_t done = nullptr;
+};
+std::mutex g_stage_mu;
+std::deque<Staging> g_stage;
+
+cudaError_t upload(void* dst, const void* src, size_t n, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cs);
+  if (e != cudaSuccess) return e;
+  // under stream capture: a plain copy (the reuse of a staging buffer is tracked with an
+  // event recorded at run time, which a captured graph does not provide)
+  if (cs != cudaStreamCaptureStatusNone) return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s);
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_stage_mu);
+  Staging* pick = nullptr;
+  for (Staging& b : g_stage) {
+    if (b.device != dev || b.bytes < n) continue;
+    const cudaError_t q = cudaEventQuery(b.done);
+    if (q == cudaErrorNotReady) {
+      if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+      continue;
+    }
+    if (q != cudaSuccess) return q;
+    pick = &b;
+    break;
+  }
+  if (!pick) {
+    Staging b;
+    b.device = dev;
+    b.bytes = std::max<size_t>((n + 65535) / 65536 * 65536, 65536);
+    if ((e = cudaHostAlloc(&b.host, b.bytes, cudaHostAllocPortable)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming)) != cudaSuccess) {
+      cudaFreeHost(b.host);
+      return e;
+    }
+    g_stage.push_back(b);
+    pick = &g_stage.back();
+  }
+  std::memcpy(pick->host, src, n);
+  if ((e = cudaMemcpyAsync(dst, pick->host, n, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  return cudaEventRecord(pick->done, s);
 }
 
 int fail(int code, const char* fmt, ...) {
@@ -700,8 +767,7 @@ int run_once(const pcg_hydro_params* p, std::vector<BoxIn>& boxes, int first, in
     cudaGetLastError();
     return fail(PCG_ENOMEM, "table allocation: %s", cudaGetErrorString(e));
   }
-  // pageable source: the copy is staged before the call returns
-  e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
+  e = upload(T.dev, T.host.data(), T.bytes, s);
   if (e == cudaSuccess) {
     bind_tables(T);
     rc = launch_stages(L, T, p, first, last, nullptr, s);
@@ -938,7 +1004,7 @@ int pcg_ctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t 
   pack_tables(L, T);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   CUDA_TRY(ws_alloc(&T.dev, T.bytes, s));
-  cudaError_t e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
+  cudaError_t e = upload(T.dev, T.host.data(), T.bytes, s);
   if (e == cudaSuccess) {
     bind_tables(T);
     pcg_hydro_params p = *prm;
@@ -1048,7 +1114,7 @@ int pcg_srctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_
   pack_tables(L, T);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   CUDA_TRY(ws_alloc(&T.dev, T.bytes, s));
-  cudaError_t e = cudaMemcpyAsync(T.dev, T.host.data(), T.bytes, cudaMemcpyHostToDevice, s);
+  cudaError_t e = upload(T.dev, T.host.data(), T.bytes, s);
   if (e == cudaSuccess) {
     bind_tables(T);
     pcg_hydro_params p = *prm;
@@ -1153,7 +1219,7 @@ int pcg_step_boxes(const pcg_hydro_params* prm, int32_t nbox, const pcg_box* box
   std::vector<char> host(off_p - off_t, 0);
   std::memcpy(host.data(), T2.host.data(), T2.bytes);
   if (!fills.empty()) std::memcpy(host.data() + (off_f - off_t), fills.data(), fills.size() * sizeof(pcg::FillBox));
-  cudaError_t e = cudaMemcpyAsync(base + off_t, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  cudaError_t e = upload(base + off_t, host.data(), host.size(), s);
   if (e != cudaSuccess) {
     cudaFreeAsync(mem, s);
     return fail(PCG_ECUDA, "table upload: %s", cudaGetErrorString(e));
@@ -1211,7 +1277,7 @@ int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t
   if (L.oversize) return fail(PCG_EINVAL, "a region needs workspace arrays of 2^31 elements or more: use smaller boxes");
   Tables T;
   pack_tables(L, T, false);
-  *bytes = int64_t((L.ws_bytes + kAlign - 1) / kAlign * kAlign + T.bytes);
+  *bytes = int64_t(size_class((L.ws_bytes + kAlign - 1) / kAlign * kAlign + T.bytes));  // as ws_alloc takes it
   return PCG_OK;
 }
 
@@ -1239,7 +1305,7 @@ int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl, dou
   std::memcpy(host.data() + b1, segs.data(), b2);
   char* dev = nullptr;
   CUDA_TRY(ws_alloc(reinterpret_cast<void**>(&dev), b1 + b2 + b3, s));
-  cudaError_t e = cudaMemcpyAsync(dev, host.data(), b1 + b2, cudaMemcpyHostToDevice, s);
+  cudaError_t e = upload(dev, host.data(), b1 + b2, s);
   rc = PCG_OK;
   if (e == cudaSuccess) {
     pcg::AuxArgs a{};
@@ -1289,7 +1355,7 @@ int pcg_update_state(int32_t nspec, int32_t nbox, const pcg_box* boxes, const pc
   std::memcpy(host.data() + b1, segs.data(), b2);
   char* dev = nullptr;
   CUDA_TRY(ws_alloc(reinterpret_cast<void**>(&dev), b1 + b2, s));
-  cudaError_t e = cudaMemcpyAsync(dev, host.data(), b1 + b2, cudaMemcpyHostToDevice, s);
+  cudaError_t e = upload(dev, host.data(), b1 + b2, s);
   if (e == cudaSuccess) {
     pcg::AuxArgs a{};
     a.boxes = reinterpret_cast<const pcg::AuxBox*>(dev);
@@ -1554,6 +1620,32 @@ int pcg_trim_workspace(int32_t device, int64_t keep_bytes) {
   if (!g_pool[device]) return PCG_OK;
   const cudaError_t e = cudaMemPoolTrimTo(g_pool[device], size_t(keep_bytes));
   if (e != cudaSuccess) return fail(PCG_ECUDA, "pool trim: %s", cudaGetErrorString(e));
+  return PCG_OK;
+}
+
+int pcg_reserve_workspace(int32_t device, int64_t bytes) {
+  if (device < 0 || device >= kMaxDevices || bytes < 0) return fail(PCG_EINVAL, "bad arguments");
+  if (bytes == 0) return PCG_OK;
+  int cur = 0;
+  CUDA_TRY(cudaGetDevice(&cur));
+  CUDA_TRY(cudaSetDevice(device));
+  // one allocation of `bytes` and its release: the pool keeps the memory (its release
+  // threshold is unbounded), and later calls carve their workspace out of it
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t s = nullptr;
+  void* p = nullptr;
+  cudaError_t e = workspace_pool(&pool);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    e = cudaMallocFromPoolAsync(&p, size_t(bytes), pool, s);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = e2;
+    cudaStreamDestroy(s);
+  }
+  cudaSetDevice(cur);
+  if (e != cudaSuccess) return fail(PCG_ECUDA, "workspace reservation of %lld bytes: %s", (long long)bytes,
+                                    cudaGetErrorString(e));
   return PCG_OK;
 }
 

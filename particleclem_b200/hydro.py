@@ -128,6 +128,16 @@ def step_boxes(prm, boxes, cfl, dt, dt_next, fill_ghosts=True, stream=None):
                 _stream_ptr(stream))
 
 
+def trim_workspace(device, keep_bytes=0):
+    """Return all but ``keep_bytes`` of the library's workspace pool of ``device`` to the driver."""
+    native.call("pcg_trim_workspace", int(device), int(keep_bytes))
+
+
+def reserve_workspace(device, nbytes):
+    """Grow the library's workspace pool of ``device`` to hold at least ``nbytes``."""
+    native.call("pcg_reserve_workspace", int(device), int(nbytes))
+
+
 def workspace_bytes(prm, extents):
     """Device bytes hydro_boxes allocates for boxes given as (lo, hi) pairs (host only)."""
     n = len(extents)

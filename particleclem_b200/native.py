@@ -62,6 +62,7 @@ SIGNATURES = {
     "pcg_step_boxes": ([_PRM, C.c_int32, _P(Box), C.c_int32, C.c_double, _V, _V, _V], C.c_int),
     "pcg_hydro_workspace": ([_PRM, C.c_int32, _P(C.c_int32), _P(C.c_int32), _P(C.c_int64)], C.c_int),
     "pcg_trim_workspace": ([C.c_int32, C.c_int64], C.c_int),
+    "pcg_reserve_workspace": ([C.c_int32, C.c_int64], C.c_int),
     "pcg_hydro_box_noalloc": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),
     "pcg_estdt": ([C.c_int32, C.c_int32, _P(Box), C.c_double, _V, _V], C.c_int),
     "pcg_update_state": ([C.c_int32, C.c_int32, _P(Box), _A4, _V, _V], C.c_int),

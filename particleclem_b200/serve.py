@@ -20,8 +20,11 @@ same time, each on its own CUDA stream, so requests that arrive while a batch ru
 the next batch and overlap it on the device. The host waits for a batch completion or the
 next arrival, whichever comes first, without polling.
 
-Latency is arrival to device completion of the request's batch (CUDA events on the
-batch's stream, on the clock of the serving start). The scheduler is device-independent:
+Latency is arrival to the host's observation of the device completion of the request's
+batch (a thread per batch blocks on the batch's CUDA event and stamps the host clock when
+it returns): the time until a client could see the result, and free of the drift between
+the GPU's event timer and the host clock over a long run. The scheduler is
+device-independent:
 an executor moves states, launches batches and keeps the clock; GpuExecutor runs them
 through the library, the CPU tests drive the scheduler with a simulated executor.
 """
@@ -207,6 +210,7 @@ class GpuExecutor:
         self.t0_event = torch.cuda.Event(enable_timing=True)
         self.t0_host = None
         self._wake = threading.Event()
+        self._finish = {}  # batch event -> host time its completion was observed
         self._pending_free = []  # (event, tensor) of evictions whose copy is in flight
 
     # ---- patches
@@ -268,6 +272,15 @@ class GpuExecutor:
         self.dev_state[pid] = None
         self.boxes[pid] = None
 
+    def reserve(self, max_inflight, max_batch_cells=None):
+        """Grow the library's workspace pool to hold ``max_inflight`` batches of at most
+        ``max_batch_cells`` cells (every patch when None), so that no batch waits for the
+        driver to map memory for a workspace size it has not seen before."""
+        per_cell = max(b / c for b, c in zip(self.nbytes, self.cells))
+        cells = sum(self.cells) if max_batch_cells is None else max_batch_cells
+        batch = max(per_cell * min(cells, sum(self.cells)), max(self.nbytes))
+        hydro.reserve_workspace(self.dev.index or 0, int(max_inflight * batch * 1.25))
+
     # ---- clock and batches
     def start(self):
         torch = self.torch
@@ -301,19 +314,20 @@ class GpuExecutor:
 
     def _watch(self, ev):
         ev.synchronize()  # blocking wait (no spinning), GIL released
+        self._finish[ev] = self.now()
         self._wake.set()
 
     def done(self, ev):
-        return ev.query()
+        return ev in self._finish  # stamped by its watcher
 
     def finish_time(self, ev):
-        return self.t0_event.elapsed_time(ev) / 1e3
+        return self._finish.pop(ev)
 
     def idle(self, next_arrival, handles):
         # sleep until a running batch completes or the next request arrives
         if self._pending_free:
             self._pending_free = [(e, t) for e, t in self._pending_free if not e.query()]
-        if handles and any(h.query() for h in handles):
+        if handles and any(self.done(h) for h in handles):
             return
         timeout = None if next_arrival is None else max(0.0, next_arrival - self.now())
         if not handles and timeout is None:
@@ -363,6 +377,8 @@ def serve_sweep(executor, pids, budget_bytes, loads=(0.1, 0.25, 0.5, 0.75, 0.8, 
 
 def _sweep(ex, pids, budget_bytes, loads, nreq, rng, seed, max_inflight, max_batch_cells, out):
     sat = None
+    if hasattr(ex, "reserve"):
+        ex.reserve(max_inflight, max_batch_cells)
     for rep, load in enumerate((math.inf, math.inf) + tuple(loads)):
         arr = np.zeros(nreq) if load is math.inf else poisson_arrivals(nreq, load * sat, seed + rep)
         choice = rng.choice(np.asarray(pids), size=nreq)
@@ -459,8 +475,8 @@ def _rel_grouped(a, b, nspec):
 
 
 def ensemble_serving(eos, nruns=16, per_run=32, seed=5, nreq=5000, budget_bytes=int(120e9),
-                     loads=(0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0), max_batch_cells=2_000_000, error_sample=32,
-                     device=0):
+                     loads=(0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0), max_batch_cells=500_000, error_sample=32,
+                     device=0, max_inflight=3):
     """The ensemble serving workload: ``nruns`` runs of ``per_run`` flame patches each with
     edges drawn from {16, 24, 32, 48, 64} (per axis, seeded per run), mixed precision,
     ``nreq`` step requests per load point on patches drawn uniformly, saturated throughput
@@ -469,9 +485,10 @@ def ensemble_serving(eos, nruns=16, per_run=32, seed=5, nreq=5000, budget_bytes=
     from . import workloads as wl
 
     patches, _ = wl.serving_patches(nruns=nruns, per_run=per_run, seed=seed, eos=eos)
-    ex = GpuExecutor(eos, precision=abi.PREC_MIXED, device=device)
+    ex = GpuExecutor(eos, precision=abi.PREC_MIXED, device=device, nstreams=max_inflight)
     pids = [ex.add_patch(p) for p in patches]
-    res = serve_sweep(ex, pids, budget_bytes, loads=loads, nreq=nreq, max_batch_cells=max_batch_cells)
+    res = serve_sweep(ex, pids, budget_bytes, loads=loads, nreq=nreq, max_batch_cells=max_batch_cells,
+                      max_inflight=max_inflight)
     resident = sum(s for _, s in ex.resident_states())
     del ex
     err = step_error(eos, patches[:error_sample], device=device)

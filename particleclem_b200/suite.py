@@ -185,7 +185,8 @@ def run_serve(args):
 
     out = ensemble_serving(wl.load_nasa7(), nruns=args.runs, per_run=args.per_run, nreq=args.requests,
                            budget_bytes=int(args.budget_gb * 1e9), loads=tuple(args.loads),
-                           max_batch_cells=args.max_batch_cells, error_sample=args.error_sample)
+                           max_batch_cells=args.max_batch_cells, error_sample=args.error_sample,
+                           max_inflight=args.max_inflight)
     for r in out["points"]:
         r.update({"workload": out["workload"], "budget_gb": args.budget_gb, "precision": "mixed"})
         print(json.dumps(r), flush=True)
@@ -267,7 +268,8 @@ def main(argv=None):
     v.add_argument("--budget-gb", type=float, default=120.0)
     v.add_argument("--loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 0.8, 0.9, 1.0])
     v.add_argument("--requests", type=int, default=5000, help="step requests per load point")
-    v.add_argument("--max-batch-cells", type=int, default=2_000_000)
+    v.add_argument("--max-batch-cells", type=int, default=500_000)
+    v.add_argument("--max-inflight", type=int, default=3)
     v.add_argument("--error-sample", type=int, default=32)
     t = sub.add_parser("step")
     t.add_argument("--level", choices=("flame", "turbulence"), default="flame")

@@ -116,12 +116,15 @@ def test_summary_percentiles():
 
 
 def test_workspace_query_is_host_only_and_additive():
+    """The query answers without a device, and the bytes of two boxes together are the
+    sum of their bytes alone up to the size classes the allocation is rounded to (from
+    1 MiB on at most 25 % above the exact size)."""
     for prec in (abi.PREC_FP64, abi.PREC_MIXED):
         prm = abi.make_params((1, 1, 1), 0.0, 9, (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), precision_mode=prec)
         a = hydro.workspace_bytes(prm, [((0, 0, 0), (31, 31, 31))])
         b = hydro.workspace_bytes(prm, [((0, 0, 0), (15, 23, 7))])
         ab = hydro.workspace_bytes(prm, [((0, 0, 0), (31, 31, 31)), ((0, 0, 0), (15, 23, 7))])
-        assert 0 < b < a and abs(ab - (a + b)) <= 4096
+        assert 0 < b < a and 0.8 * (a + b) <= ab <= 1.25 * (a + b)
         # at least the traced states: 2 x 3 directions x (6+NS) values per cell of grow(box,1)
         assert a >= 6 * 15 * 34 ** 3 * (4 if prec == abi.PREC_MIXED else 8)
     m = hydro.workspace_bytes(abi.make_params((1, 1, 1), 0.0, 9, (0,) * 3, (0,) * 3, (0,) * 3, (0,) * 3,

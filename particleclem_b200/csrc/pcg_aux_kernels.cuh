@@ -93,11 +93,11 @@ __global__ void __launch_bounds__(128) k_estdt_final(pcg::AuxArgs a) {
 // Source/Advance.cpp:397-417 (construct_Snew, hydro only) then Source/PeleC.cpp:2289-2305
 // (computeTemp): pc_rst_int_e default branch (PeleCUtilities.H:227-235) and pc_cmpTemp
 // (PeleCUtilities.H:70-84), on one cell: s holds S_old on entry and S_new on exit.
+// construct_Snew's pc_rst_int_e and computeTemp on the state s (already S_old + dt *
+// hydro source).
 template <int NS, bool MIX>
-__device__ __forceinline__ void update_cell(double* s, const double* hsrc, double dt) {
+__device__ __forceinline__ void finish_cell(double* s) {
   using E = Eos<NS, MIX, double>;
-#pragma unroll
-  for (int n = 0; n < pcg::nvar(NS); ++n) s[n] += dt * hsrc[n];
   const double rho = s[pcg::URHO];
   const double rhoInv = 1.0 / rho;
   const double Up = s[pcg::UMX] * rhoInv;
@@ -111,6 +111,13 @@ __device__ __forceinline__ void update_cell(double* s, const double* hsrc, doubl
 #pragma unroll
   for (int n = 0; n < NS; ++n) y[n] = s[pcg::UFS + n] * rhoInv2;
   s[pcg::UTEMP] = E::rey2t(e, y, s[pcg::UTEMP]);
+}
+
+template <int NS, bool MIX>
+__device__ __forceinline__ void update_cell(double* s, const double* hsrc, double dt) {
+#pragma unroll
+  for (int n = 0; n < pcg::nvar(NS); ++n) s[n] += dt * hsrc[n];
+  finish_cell<NS, MIX>(s);
 }
 
 template <int NS, bool MIX>
@@ -145,15 +152,17 @@ __global__ void __launch_bounds__(128, MINB) k_advance(pcg::StageArgs a) {
   double dtc = DBL_MAX;
   if (item_of(a, it)) {
     const pcg::Region& rg = *it.rg;
-    double h[pcg::nvar(NS)], s[pcg::nvar(NS)];
-    if (rg.ff_single)
-      consup_sum<NS, float>(rg, it.i, it.j, it.k, p0_of<NS, MIX, float>(rg), h);
-    else
-      consup_sum<NS, double>(rg, it.i, it.j, it.k, 0.0, h);
+    double s[pcg::nvar(NS)];
     const CellPtr<double> u = at(v4<double>(rg.uin), it.i, it.j, it.k);
-#pragma unroll
-    for (int n = 0; n < pcg::nvar(NS); ++n) s[n] = u[n];
-    update_cell<NS, MIX>(s, h, dt_of(a, rg));
+    const double dt = dt_of(a, rg);
+    // S_old + dt * hydro source, each component as its source is formed (the source
+    // itself is never held whole)
+    const auto add = [&](int n, double hn) { s[n] = u[n] + dt * hn; };
+    if (rg.ff_single)
+      consup_each<NS, float>(rg, it.i, it.j, it.k, p0_of<NS, MIX, float>(rg), add);
+    else
+      consup_each<NS, double>(rg, it.i, it.j, it.k, 0.0, add);
+    finish_cell<NS, MIX>(s);
 #pragma unroll
     for (int n = 0; n < pcg::nvar(NS); ++n) u[n] = s[n];
     dtc = cfl_dt<NS, MIX>(s, rg.dx);

@@ -1678,8 +1678,11 @@ template <> struct FinalView<float> {
   }
 };
 
-template <int NS, class F>
-__device__ __forceinline__ void consup_sum(const pcg::Region& rg, int i, int j, int k, double p0, double* h) {
+// The hydro source of cell (i, j, k), component by component: out(n, h_n) for n = 0 ..
+// NVAR-1 (the p div u term already in h_UEINT), so that a caller can consume each
+// component as it is formed instead of holding all of them.
+template <int NS, class F, class OUT>
+__device__ __forceinline__ void consup_each(const pcg::Region& rg, int i, int j, int k, double p0, OUT&& out) {
   using FV = FinalView<F>;
   typename FV::C f0, f0p, f1, f1p, f2, f2p, q0, q0p, q1, q1p, q2, q2p;
   FV::cells(rg.ff[0], 0, i, j, k, f0, f0p);
@@ -1705,11 +1708,17 @@ __device__ __forceinline__ void consup_sum(const pcg::Region& rg, int i, int j, 
 #pragma unroll
   for (int n = 0; n < pcg::nvar(NS); ++n) {
     const double old = rg.zero_uout ? 0.0 : uo[n];
-    h[n] = old + (double(f0[n]) - double(f0p[n]) + double(f1[n]) - double(f1p[n]) + double(f2[n]) -
-                  double(f2p[n])) /
-                     v;
+    double h = old + (double(f0[n]) - double(f0p[n]) + double(f1[n]) - double(f1p[n]) + double(f2[n]) -
+                      double(f2p[n])) /
+                         v;
+    if (n == pcg::UEINT) h -= pdivu;
+    out(n, h);
   }
-  h[pcg::UEINT] -= pdivu;
+}
+
+template <int NS, class F>
+__device__ __forceinline__ void consup_sum(const pcg::Region& rg, int i, int j, int k, double p0, double* h) {
+  consup_each<NS, F>(rg, i, j, k, p0, [&](int n, double hn) { h[n] = hn; });
 }
 
 template <int NS, class F>

@@ -239,8 +239,13 @@ def run_step(args):
 
     from .level import LevelStepper
 
+    from . import autotune
+
     lev = wl.flame(n=args.n, box=args.box, seed=2) if args.level == "flame" else wl.turbulence(n=args.n, box=args.box)
     prec = {"mixed": abi.PREC_MIXED, "fp64": abi.PREC_FP64, "fast": abi.PREC_FP64_FAST}[args.form]
+    for sv in args.variant:  # launch variants to profile, stage=variant (autotune.STAGE_NAMES)
+        name, v = sv.split("=")
+        autotune.set_variant(prec, lev.nspec, autotune.STAGE_NAMES.index(name), int(v))
     st = LevelStepper(lev, precision=prec, fuse=not args.per_box, ppm_type=args.ppm)
     for _ in range(args.steps):
         st.step()
@@ -276,6 +281,7 @@ def main(argv=None):
     t.add_argument("--n", type=int, default=64)
     t.add_argument("--box", type=int, default=32)
     t.add_argument("--form", choices=("mixed", "fp64", "fast"), default="mixed")
+    t.add_argument("--variant", nargs="*", default=[], help="launch variants, e.g. trace=5")
     t.add_argument("--ppm", type=int, default=1)
     t.add_argument("--per-box", action="store_true", help="advance the boxes as separate regions")
     t.add_argument("--steps", type=int, default=2)

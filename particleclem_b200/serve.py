@@ -272,14 +272,18 @@ class GpuExecutor:
         self.dev_state[pid] = None
         self.boxes[pid] = None
 
-    def reserve(self, max_inflight, max_batch_cells=None):
+    def reserve(self, max_inflight, max_batch_cells=None, cap_bytes=None):
         """Grow the library's workspace pool to hold ``max_inflight`` batches of at most
-        ``max_batch_cells`` cells (every patch when None), so that no batch waits for the
-        driver to map memory for a workspace size it has not seen before."""
+        ``max_batch_cells`` cells (every patch when None), at most ``cap_bytes``, so that no
+        batch waits for the driver to map memory for a workspace size it has not seen
+        before."""
         per_cell = max(b / c for b, c in zip(self.nbytes, self.cells))
         cells = sum(self.cells) if max_batch_cells is None else max_batch_cells
         batch = max(per_cell * min(cells, sum(self.cells)), max(self.nbytes))
-        hydro.reserve_workspace(self.dev.index or 0, int(max_inflight * batch * 1.25))
+        nbytes = int(max_inflight * batch * 1.25)
+        if cap_bytes is not None:
+            nbytes = min(nbytes, int(cap_bytes))
+        hydro.reserve_workspace(self.dev.index or 0, nbytes)
 
     # ---- clock and batches
     def start(self):
@@ -378,7 +382,7 @@ def serve_sweep(executor, pids, budget_bytes, loads=(0.1, 0.25, 0.5, 0.75, 0.8, 
 def _sweep(ex, pids, budget_bytes, loads, nreq, rng, seed, max_inflight, max_batch_cells, out):
     sat = None
     if hasattr(ex, "reserve"):
-        ex.reserve(max_inflight, max_batch_cells)
+        ex.reserve(max_inflight, max_batch_cells, cap_bytes=budget_bytes)
     for rep, load in enumerate((math.inf, math.inf) + tuple(loads)):
         arr = np.zeros(nreq) if load is math.inf else poisson_arrivals(nreq, load * sat, seed + rep)
         choice = rng.choice(np.asarray(pids), size=nreq)

@@ -73,3 +73,30 @@ def test_copy_cells_argument_errors():
     assert rc(a, c, (0, 0, 0), (3, 3, 3)) == -1
     assert "dst must cover" in native.load().pcg_last_error().decode()
     assert rc(a, a, (2, 2, 2), (1, 5, 5)) == -1
+
+
+def test_workspace_pool_argument_errors():
+    """pcg_reserve_workspace and pcg_trim_workspace reject bad devices and sizes with
+    PCG_EINVAL before any device work; reserving nothing is a no-op."""
+    assert _rc("pcg_reserve_workspace", -1, 0) == -1
+    assert _rc("pcg_reserve_workspace", 0, -5) == -1
+    assert _rc("pcg_reserve_workspace", 0, 0) == 0
+    assert _rc("pcg_trim_workspace", -1, 0) == -1
+    assert _rc("pcg_trim_workspace", 0, -1) == -1
+
+
+def test_tiled_trace_variants_only_for_the_mixed_trace():
+    """Launch variants 3-5 (the TMA-staged tiled trace) exist for the mixed form's trace
+    only; every other (form, stage) takes 0-2."""
+    from particleclem_b200 import autotune
+
+    saved = autotune.get_variant(abi.PREC_MIXED, 9, autotune.TRACE_STAGE)
+    try:
+        assert _rc("pcg_set_launch_variant", abi.PREC_MIXED, 9, autotune.TRACE_STAGE, 5) == 0
+        assert autotune.get_variant(abi.PREC_MIXED, 9, autotune.TRACE_STAGE) == 5
+        assert _rc("pcg_set_launch_variant", abi.PREC_MIXED, 9, autotune.TRACE_STAGE, 6) == -1
+        assert _rc("pcg_set_launch_variant", abi.PREC_FP64, 9, autotune.TRACE_STAGE, 3) == -1
+        assert _rc("pcg_set_launch_variant", abi.PREC_MIXED, 9, 3, 3) == -1  # flux0
+    finally:
+        autotune.set_variant(abi.PREC_MIXED, 9, autotune.TRACE_STAGE, saved)
+    assert autotune.describe(abi.PREC_MIXED, autotune.TRACE_STAGE, 4).startswith("TMA-staged tiles")

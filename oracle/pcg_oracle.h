@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define ORC_MAXNS 16
+#define ORC_MAXNS 64
 
 typedef struct {
   double* p;

@@ -1,16 +1,18 @@
 // pcg_dispatch.cuh -- per-translation-unit launch entry points. Each kernel translation
-// unit instantiates the stage kernels for ONE species count (PCG_TU_NS, 1 or 9) and one
+// unit instantiates the stage kernels for ONE species count (PCG_TU_NS) and one
 // arithmetic: PCG_TU_DOUBLE_ONLY (FP64 reference order, compiled --fmad=false),
 // PCG_TU_SINGLE_ONLY (the mixed form's FP32 stage kernels) or neither (FP64 with FMA
 // contraction, and the FP64 step tail of both fast forms). Each unit has its own
-// PCG_TU namespace and its own copy of the EOS constant bank; the host routes a call to
-// the unit of its (precision form, species count).
+// PCG_TU namespace and its own copy of the EOS constant bank, and registers itself with
+// the host (pcg_units.h), which routes a call to the unit of its (precision form,
+// species count).
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include "pcg_kernels.cuh"
 #include "pcg_aux_kernels.cuh"
+#include "pcg_units.h"
 
 #ifndef PCG_TU_NS
 #error "PCG_TU_NS (species count of this translation unit) must be defined"
@@ -68,7 +70,7 @@ static cudaError_t launch_special(int stage, const pcg::StageArgs& a, const dim3
 template <int NS, bool MIX, class R>
 static cudaError_t launch_trace_tile(const pcg::StageArgs& a, const dim3& grid, const dim3& block, int variant,
                                     cudaStream_t s) {
-  if constexpr (sizeof(R) == 4) {
+  if constexpr (sizeof(R) == 4 && pcg::trace_tile_species(NS)) {
     switch (variant) {
       case 0: k_trace_tile<NS, MIX, kMinBlocks[K_TRACE][0]><<<grid, block, 0, s>>>(a); break;
       case 1: k_trace_tile<NS, MIX, kMinBlocks[K_TRACE][1]><<<grid, block, 0, s>>>(a); break;
@@ -77,7 +79,7 @@ static cudaError_t launch_trace_tile(const pcg::StageArgs& a, const dim3& grid, 
     }
     return cudaGetLastError();
   } else {
-    return cudaErrorInvalidValue;  // the FP64 forms trace from the global array
+    return cudaErrorInvalidValue;  // the FP64 forms and large species counts trace per cell
   }
 }
 
@@ -96,7 +98,7 @@ static cudaError_t launch_t(int stage, const pcg::StageArgs& a, int64_t nblocks,
   }
 }
 
-// ns: species count (1: gamma law, 9: NASA-7 mixture); single: FP32 compute type. A
+// ns: species count (1: gamma law, more: NASA-7 mixture); single: FP32 compute type. A
 // combination this unit does not hold is cudaErrorInvalidValue.
 constexpr int kNS = PCG_TU_NS;
 constexpr bool kMix = PCG_TU_NS > 1;
@@ -129,5 +131,27 @@ cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks
   return launch_aux_t<kNS, kMix>(which, a, nblocks, s);
 }
 #endif
+
+// Registration with the host's unit table at library load.
+struct UnitRegistration {
+  UnitRegistration() {
+    pcg::UnitEntry u{};
+    u.ns = kNS;
+    u.upload_eos = &upload_eos;
+    u.launch_stage = &launch_stage;
+#if defined(PCG_TU_DOUBLE_ONLY)
+    u.kind = pcg::UNIT_STRICT;
+    u.launch_advance = &launch_advance;
+    u.launch_aux = &launch_aux;
+#elif defined(PCG_TU_SINGLE_ONLY)
+    u.kind = pcg::UNIT_MIXED;
+#else
+    u.kind = pcg::UNIT_FAST;
+    u.launch_advance = &launch_advance;
+#endif
+    pcg::register_unit(u);
+  }
+};
+static UnitRegistration g_unit_registration;
 
 }  // namespace PCG_TU

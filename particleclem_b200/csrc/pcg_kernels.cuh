@@ -818,6 +818,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace_tile(pcg::StageArgs a) {
   __shared__ float dsv[NE * kDsv];  // van Leer slopes (PPM)
   __shared__ float edg[NE * kEdg];  // interface values (PPM)
   __shared__ __align__(8) uint64_t bar;
+  static_assert(sizeof(tile) + sizeof(dsv) + sizeof(edg) + 8 <= 48 * 1024, "tile shared memory");
   int t;
   const pcg::Seg& sg = seg_of(a, t);
   if (sg.variant < 3) {  // a strip: one cell per thread (the block's segment is uniform)
@@ -1517,6 +1518,14 @@ __device__ __forceinline__ void flux2_x(const pcg::StageArgs& a, const pcg::Seg&
   flux2_face<NS, MIX, EXACT, 0, R, UMETH>(a, rg, i, j, k, ql, qr, p0d);
 }
 
+// Shared-memory correction slots of a k_flux2 thread: two (the march below) while they
+// fit the 48 KB of static shared memory of a block, else one (large species counts in
+// FP64), with the correction of the cell behind the face swapped through it.
+template <int NS, class R>
+__host__ __device__ constexpr int flux2_slots() {
+  return 2 * ncorr<NS>() * 128 * int(sizeof(R)) <= 48 * 1024 ? 2 : 1;
+}
+
 template <int NS, bool MIX, bool EXACT, int D, class R, bool UMETH = false>
 __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::Seg& sg, int t, R* kcarry) {
   const pcg::Region& rg = a.regions[sg.region];
@@ -1526,6 +1535,30 @@ __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::
   double p0d;
   flux2_consts<NS, MIX, EXACT, R>(a, rg, D, cdtdx0, cdtdx1, hdt, p0d);
   const R p0 = R(p0d);
+  if constexpr (flux2_slots<NS, R>() == 1) {
+    R* sl = kcarry + threadIdx.x;
+    R K[ncorr<NS>()];
+    if (D == 1)
+      flux2_corr<NS, D, R>(rg, i, m0 - 1, r, cdtdx0, cdtdx1, p0, K);
+    else
+      flux2_corr<NS, D, R>(rg, i, r, m0 - 1, cdtdx0, cdtdx1, p0, K);
+#pragma unroll
+    for (int n = 0; n < ncorr<NS>(); ++n) sl[n * 128] = K[n];
+    for (int m = m0; m < m1; ++m) {
+      const int j = (D == 1) ? m : r, k = (D == 1) ? r : m;
+      flux2_corr<NS, D, R>(rg, i, j, k, cdtdx0, cdtdx1, p0, K);
+      R ql[pcg::nt_comps(NS)], qr[pcg::nt_comps(NS)];
+      flux2_state<NS, EXACT, D, 1, R>(rg, i, j, k, K, hdt, p0, qr);
+#pragma unroll
+      for (int n = 0; n < ncorr<NS>(); ++n) {
+        const R kl = sl[n * 128];
+        sl[n * 128] = K[n];
+        K[n] = kl;
+      }
+      flux2_state<NS, EXACT, D, 0, R>(rg, i, j, k, K, hdt, p0, ql);
+      flux2_face<NS, MIX, EXACT, D, R, UMETH>(a, rg, i, j, k, ql, qr, p0d);
+    }
+  } else {
   // the correction of the cell behind the face waits in one of this thread's two
   // shared-memory slots (component-major, conflict free): each step first forms the
   // correction of the next cell with nothing else live, then corrects both states
@@ -1553,11 +1586,12 @@ __device__ __forceinline__ void flux2_march(const pcg::StageArgs& a, const pcg::
     sr = tmp;
     flux2_face<NS, MIX, EXACT, D, R, UMETH>(a, rg, i, j, k, ql, qr, p0d);
   }
+  }
 }
 
 template <int NS, bool MIX, bool EXACT, class R, int MINB, bool UMETH = false>
 __global__ void __launch_bounds__(128, MINB) k_flux2(pcg::StageArgs a) {
-  __shared__ R kcarry[2 * ncorr<NS>() * 128];
+  __shared__ R kcarry[flux2_slots<NS, R>() * ncorr<NS>() * 128];
   int t;
   const pcg::Seg& sg = seg_of(a, t);
   switch (sg.variant) {

@@ -1,6 +1,6 @@
 // The mixed form's stage kernels (PCG_PREC_MIXED): FP32 trace, Riemann and transverse
 // arithmetic, FP64 state, ctoprim Newton solve and flux accumulation. Built once per
-// species count into pcg_mixed1 / pcg_mixed9, with FMA contraction and the approximate
+// species count of the build (namespace pcg_mixed<n>), with FMA contraction and the approximate
 // FP32 division and square root.
 #define PCG_CAT2(a, b) a##b
 #define PCG_CAT(a, b) PCG_CAT2(a, b)

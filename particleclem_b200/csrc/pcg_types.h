@@ -41,7 +41,14 @@ constexpr double RU = 8.31446261815324e7;
 constexpr int NEWTON_MAXIT = 20;
 constexpr double NEWTON_RTOL = 1.0e-10;
 constexpr double NEWTON_TMIN = 10.0;
-constexpr int MAXNS = 16;
+// Largest species count of an EOS table (the bank size of the constant-memory EOS
+// tables, even so that species pairs fill it). The build sets it from the largest
+// species count it compiles kernels for; every unit and the host see the same value.
+#ifndef PCG_MAXNS
+#define PCG_MAXNS 16
+#endif
+constexpr int MAXNS = PCG_MAXNS;
+static_assert(MAXNS % 2 == 0, "PCG_MAXNS must be even");
 // The kernels address a view with 32-bit element offsets: every view the host passes them
 // (workspace arrays and the caller's arrays) spans fewer elements than this.
 constexpr int64_t kMaxViewElems = 2147483647;
@@ -177,6 +184,10 @@ PCG_HD constexpr int trace_box_x(int d) { return d == 0 ? 40 : 36; }
 PCG_HD constexpr int trace_box_y(int d) { return d == 0 ? 4 : d == 1 ? 8 : 1; }
 PCG_HD constexpr int trace_box_z(int d) { return d == 2 ? 8 : 1; }
 PCG_HD constexpr int trace_box_cells(int d) { return trace_box_x(d) * trace_box_y(d) * trace_box_z(d); }
+// The tiled trace's shared arrays (the staged primitives, slopes and interface values of
+// a tile) grow with the species count: about 37 KB at 9 species, past 12 species more
+// than the 48 KB of static shared memory of a block. Larger counts trace per cell.
+PCG_HD constexpr bool trace_tile_species(int ns) { return ns <= 12; }
 // Bytes of one CUtensorMap (the layout of the driver's opaque type).
 constexpr int kTensorMapBytes = 128;
 

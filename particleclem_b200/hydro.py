@@ -40,6 +40,15 @@ def init(device: int = 0):
     native.call("pcg_init", int(device))
 
 
+def species_counts():
+    """The species counts the loaded library has kernels for (ascending)."""
+    lib = native.load()
+    n = lib.pcg_species_counts(None, 0)
+    buf = (C.c_int32 * max(n, 1))()
+    lib.pcg_species_counts(buf, n)
+    return tuple(int(buf[k]) for k in range(n))
+
+
 def set_eos(eos):
     """Upload an EOS table (GammaLaw or Nasa7Mixture) to the library."""
     if isinstance(eos, GammaLaw):

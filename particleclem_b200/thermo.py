@@ -83,3 +83,30 @@ def load_nasa7(path: str = STANDIN_TABLE) -> Nasa7Mixture:
         lo.append([float(v) for v in lines[3 * s + 1].split()])
         hi.append([float(v) for v in lines[3 * s + 2].split()])
     return Nasa7Mixture(tuple(names), np.array(mw), np.array(tmid), np.array(lo), np.array(hi))
+
+
+def standin_mixture(nspec: int, base: Nasa7Mixture = None) -> Nasa7Mixture:
+    """A NASA-7 table of ``nspec`` species (2 or more) built from the 9-species stand-in,
+    for exercising species counts other than 9 (mechanisms of 2, 3 or 21 species have
+    those sizes). It is a synthetic table, not a real mechanism: up to
+    9 species it is the first ``nspec - 1`` stand-in species plus N2; above 9, the nine
+    plus species whose polynomials repeat the stand-in's (cycling through them) with the
+    molecular weight scaled by 1 + 0.1 m for the m-th repeat, so that every species has
+    distinct thermodynamics in mass units."""
+    base = base or load_nasa7()
+    if nspec < 2:
+        raise ValueError("a mixture has 2 or more species")
+    if nspec <= base.nspec:
+        idx = list(range(nspec - 1)) + [base.nspec - 1]
+        return Nasa7Mixture(tuple(base.names[k] for k in idx), base.mw[idx].copy(), base.tmid[idx].copy(),
+                            base.a_lo[idx].copy(), base.a_hi[idx].copy())
+    names, mw, tmid, lo, hi = list(base.names), list(base.mw), list(base.tmid), list(base.a_lo), list(base.a_hi)
+    for m in range(nspec - base.nspec):
+        k = m % base.nspec
+        names.append(f"{base.names[k]}_x{m + 1}")
+        mw.append(base.mw[k] * (1.0 + 0.1 * (m + 1)))
+        tmid.append(base.tmid[k])
+        lo.append(base.a_lo[k])
+        hi.append(base.a_hi[k])
+    return Nasa7Mixture(tuple(names), np.array(mw), np.array(tmid), np.array(lo), np.array(hi))
+

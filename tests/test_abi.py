@@ -100,3 +100,25 @@ def test_tiled_trace_variants_only_for_the_mixed_trace():
     finally:
         autotune.set_variant(abi.PREC_MIXED, 9, autotune.TRACE_STAGE, saved)
     assert autotune.describe(abi.PREC_MIXED, autotune.TRACE_STAGE, 4).startswith("TMA-staged tiles")
+
+
+def test_species_counts_of_the_build():
+    """pcg_species_counts lists the species counts the library was compiled for (the
+    build's PCG_NSPEC list); a mixture table or a call for any other count is refused with
+    PCG_EUNSUPPORTED before any device work, and a one-species NASA-7 table with
+    PCG_EINVAL (one species is the gamma law)."""
+    import numpy as np
+
+    from particleclem_b200 import build, hydro
+
+    counts = hydro.species_counts()
+    assert counts == build.species_counts()
+    assert 1 in counts and 9 in counts
+    missing = next(n for n in range(2, 64) if n not in counts)
+    tab = [np.ones(7 * missing) for _ in range(4)]
+    ptrs = [t.ctypes.data_as(C.POINTER(C.c_double)) for t in tab]
+    assert _rc("pcg_set_eos_nasa7", missing, *ptrs) == -4
+    assert str(missing) in native.load().pcg_last_error().decode()
+    assert _rc("pcg_set_eos_nasa7", 1, *ptrs) == -1
+    prm = abi.make_params((1, 1, 1), 0.1, missing, (0, 0, 0), (7, 7, 7), (0, 0, 0), (0, 0, 0))
+    assert _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), None, None, None, None) == -4

@@ -41,7 +41,7 @@ enum {
   PCG_EINVAL = -1,       /* bad argument (box, array extent, parameter) */
   PCG_ECUDA = -2,        /* a CUDA runtime call failed */
   PCG_ENOMEM = -3,       /* device allocation failed */
-  PCG_EUNSUPPORTED = -4, /* option not implemented (nspec other than 1 or 9) */
+  PCG_EUNSUPPORTED = -4, /* option not implemented (a species count this build has no kernels for) */
   PCG_ETIMEDOUT = -5,    /* a bounded device wait gave up */
   PCG_EBUDGET = -6,      /* serving: request exceeds the memory budget */
   PCG_ENOEOS = -7        /* no EOS table set for this species count */
@@ -80,7 +80,7 @@ typedef struct pcg_hydro_params {
   int32_t weno_scheme;     /* with use_hybrid_weno: 0 WENO-JS5, 1 WENO-Z5, 2 WENO-Z7, 3 WENO-Z3 */
   int32_t domlo[3], domhi[3];
   int32_t bclo[3], bchi[3];
-  int32_t nspec;          /* NUM_SPECIES: 1 (gamma law) or 9 (NASA-7 mixture) */
+  int32_t nspec;          /* NUM_SPECIES: 1 (gamma law) or a mixture count of the build (pcg_species_counts) */
   int32_t precision_mode; /* PCG_PREC_* */
 } pcg_hydro_params;
 
@@ -110,9 +110,17 @@ int pcg_init(int device);
  * restatement). Gamma law: one species, constant gamma, molecular weight mw. */
 int pcg_set_eos_gamma(double gamma, double mw);
 /* Ideal-gas mixture with NASA-7 polynomials: a_lo/a_hi hold 7 coefficients per
- * species (HOST pointers), tmid the range split per species. */
+ * species (HOST pointers), tmid the range split per species. nspec: 2 or more, one of
+ * the build's species counts (PCG_EUNSUPPORTED otherwise). One mixture table is active
+ * at a time. */
 int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid,
                       const double* a_lo, const double* a_hi);
+/* The species counts this build has kernels for. The reference's NUM_SPECIES is a
+ * compile-time constant of its mechanism (Source/IndexDefines.H:50-89); the library is
+ * compiled for a list of them (particleclem_b200/build.py, PCG_NSPEC; 1 is the gamma
+ * law). Writes up to max_counts of them, ascending, into counts (which may be NULL)
+ * and returns how many there are. Host only: no device is touched. */
+int pcg_species_counts(int32_t* counts, int32_t max_counts);
 
 const char* pcg_last_error(void);
 
@@ -284,6 +292,48 @@ int pcg_trim_workspace(int32_t device, int64_t keep_bytes);
  * otherwise wait for the driver to map memory (tens to hundreds of milliseconds
  * measured on B200). No counterpart in the reference. */
 int pcg_reserve_workspace(int32_t device, int64_t bytes);
+
+/* ---- coarse/fine: flux register, reflux, average-down ---------------------------- */
+
+/* The coarse/fine use of the exported fluxes (Source/Hydro.cpp:281-287 ->
+ * PeleC::update_flux_registers, Source/PeleC.cpp:1343-1400; PeleC::reflux,
+ * Source/PeleC.cpp:1403-1414; the register class is AMReX's EBFluxRegister on regular
+ * boxes, whose CrseAdd / FineAdd / Reflux these calls replace). A register sits between
+ * a coarse level (domain crse_domlo..crse_domhi, periodic[d] != 0 where periodic) and
+ * the fine boxes above it (fine index space, refinement ratio `ratio` in every
+ * direction, boxes aligned to the ratio, inside the coarse domain, disjoint). It holds
+ * one accumulator of ncomp doubles per coarse face on the coarse/fine boundary (faces on
+ * non-periodic domain boundaries and between fine boxes have none). All calls are on the
+ * device current at creation; the register owns its device memory. */
+typedef struct pcg_fluxreg pcg_fluxreg;
+int pcg_fluxreg_create(int32_t ncomp, const int32_t crse_domlo[3], const int32_t crse_domhi[3],
+                       const int32_t periodic[3], int32_t ratio, int32_t nfine, const int32_t* fine_lo /*[3*nfine]*/,
+                       const int32_t* fine_hi /*[3*nfine]*/, pcg_fluxreg** out);
+/* nfaces: accumulators (coarse/fine faces); ncells: coarse cells they correct. Host only. */
+int pcg_fluxreg_info(const pcg_fluxreg* reg, int32_t* nfaces, int32_t* ncells);
+/* Zero the accumulators (start of the coarse step, Source/Advance.cpp:30-31). */
+int pcg_fluxreg_reset(pcg_fluxreg* reg, pcg_stream_t stream);
+/* CrseAdd: coarse box [lo, hi] with its area-weighted fluxes flx[3] (the flx export of
+ * pcg_box / pcg_hydro_box, d-faces lo..hi+1) of a step of dt: every register face of a
+ * coarse cell in the box takes -s * dt * F (s = +1 on the cell's low face, -1 on its
+ * high face). */
+int pcg_fluxreg_crse_add(pcg_fluxreg* reg, const int32_t lo[3], const int32_t hi[3], const pcg_array4* flx /*[3]*/,
+                         double dt, pcg_stream_t stream);
+/* FineAdd: fine box [lo, hi] (one of the register's) with its area-weighted fluxes of a
+ * fine step of dt: every register face it borders takes +s * dt * (the sum of its ratio^2
+ * fine faces). Called once per fine box and fine substep. */
+int pcg_fluxreg_fine_add(pcg_fluxreg* reg, const int32_t lo[3], const int32_t hi[3], const pcg_array4* flx /*[3]*/,
+                         double dt, pcg_stream_t stream);
+/* Reflux: S += (sum of the cell's accumulators) / vol on every coarse cell next to the
+ * fine region (vol: the coarse cell volume). The caller recomputes T afterwards, as
+ * PeleC's post_timestep does. */
+int pcg_fluxreg_reflux(pcg_fluxreg* reg, pcg_array4* s_crse, double vol, pcg_stream_t stream);
+int pcg_fluxreg_destroy(pcg_fluxreg* reg);
+/* avgDown on regular boxes (PeleC::avgDown, Source/PeleC.cpp after :1091; AMReX's
+ * average_down): every coarse cell under the fine box [fine_lo, fine_hi] becomes the mean
+ * of its ratio^3 fine cells, components 0..ncomp-1. */
+int pcg_average_down(const pcg_array4* fine, pcg_array4* crse, const int32_t fine_lo[3], const int32_t fine_hi[3],
+                     int32_t ratio, int32_t ncomp, pcg_stream_t stream);
 
 /* ---- launch tuning ------------------------------------------------------------- */
 

@@ -26,67 +26,89 @@
 #include "../../include/pcg_hydro.h"
 #include "pcg_types.h"
 
-// The kernel translation units, one per (arithmetic, species count): see pcg_dispatch.cuh.
-#define PCG_DECL_TU(NAME)                                                                              \
-  namespace NAME {                                                                                     \
-  cudaError_t upload_eos(int slot, const pcg::EosConst& e);                                            \
-  cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks,  \
-                           int variant, cudaStream_t s);                                               \
-  }
-PCG_DECL_TU(pcg_strict1)
-PCG_DECL_TU(pcg_strict9)
-PCG_DECL_TU(pcg_fast1)
-PCG_DECL_TU(pcg_fast9)
-PCG_DECL_TU(pcg_mixed1)
-PCG_DECL_TU(pcg_mixed9)
-#undef PCG_DECL_TU
-#define PCG_DECL_ADV(NAME) \
-  namespace NAME { cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s); }
-PCG_DECL_ADV(pcg_strict1)
-PCG_DECL_ADV(pcg_strict9)
-PCG_DECL_ADV(pcg_fast1)
-PCG_DECL_ADV(pcg_fast9)
-#undef PCG_DECL_ADV
-namespace pcg_strict1 { cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s); }
-namespace pcg_strict9 { cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s); }
+#include "pcg_units.h"
+
+// The kernel translation units, one per (arithmetic, species count), register their
+// entry points here at library load (pcg_dispatch.cuh); the table is written only by
+// those static initialisers and read afterwards.
+namespace pcg {
+namespace {
+struct UnitTable {
+  std::vector<UnitEntry> units;
+};
+UnitTable& unit_table() {
+  static UnitTable t;
+  return t;
+}
+}  // namespace
+void register_unit(const UnitEntry& u) { unit_table().units.push_back(u); }
+}  // namespace pcg
+
+namespace {
+const pcg::UnitEntry* find_unit(int kind, int ns) {
+  for (const pcg::UnitEntry& u : pcg::unit_table().units)
+    if (u.kind == kind && u.ns == ns) return &u;
+  return nullptr;
+}
+// true when the build holds the kernels of every form for this species count
+bool species_built(int ns) {
+  return find_unit(pcg::UNIT_STRICT, ns) && find_unit(pcg::UNIT_FAST, ns) && find_unit(pcg::UNIT_MIXED, ns);
+}
+// the species counts with kernels, ascending, as text ("1, 9")
+std::string species_list() {
+  std::vector<int> v;
+  for (const pcg::UnitEntry& u : pcg::unit_table().units)
+    if (u.kind == pcg::UNIT_STRICT && species_built(u.ns)) v.push_back(u.ns);
+  std::sort(v.begin(), v.end());
+  std::string out;
+  for (size_t k = 0; k < v.size(); ++k) out += (k ? ", " : "") + std::to_string(v[k]);
+  return out;
+}
+}  // namespace
 
 // Routing by species count: pcg_strict = FP64 reference order (and the FP64 auxiliary
 // kernels), pcg_fast = FMA-contracted FP64 stages (single == false) or the mixed form's
-// FP32 stages (single == true), and the FP64 step tail of both fast forms.
+// FP32 stages (single == true), and the FP64 step tail of both fast forms. A species
+// count without kernels is cudaErrorInvalidValue (the entry points refuse it earlier
+// with PCG_EUNSUPPORTED).
 namespace pcg_strict {
+// slot 0 holds the gamma law (species count 1), slot 1 the mixture table of e.nspec
+// species: each goes to the units of that species count
 cudaError_t upload_eos(int slot, const pcg::EosConst& e) {
-  return slot == 0 ? pcg_strict1::upload_eos(slot, e) : pcg_strict9::upload_eos(slot, e);
+  const pcg::UnitEntry* u = find_unit(pcg::UNIT_STRICT, slot == 0 ? 1 : e.nspec);
+  return u ? u->upload_eos(slot, e) : cudaErrorInvalidValue;
 }
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
                          cudaStream_t s) {
-  return ns == 1 ? pcg_strict1::launch_stage(stage, ns, single, a, nblocks, variant, s)
-                 : pcg_strict9::launch_stage(stage, ns, single, a, nblocks, variant, s);
+  const pcg::UnitEntry* u = find_unit(pcg::UNIT_STRICT, ns);
+  return u ? u->launch_stage(stage, ns, single, a, nblocks, variant, s) : cudaErrorInvalidValue;
 }
 cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
-  return ns == 1 ? pcg_strict1::launch_advance(ns, a, nblocks, variant, s)
-                 : pcg_strict9::launch_advance(ns, a, nblocks, variant, s);
+  const pcg::UnitEntry* u = find_unit(pcg::UNIT_STRICT, ns);
+  return u ? u->launch_advance(ns, a, nblocks, variant, s) : cudaErrorInvalidValue;
 }
 cudaError_t launch_aux(int which, int ns, const pcg::AuxArgs& a, int64_t nblocks, cudaStream_t s) {
-  return ns == 1 ? pcg_strict1::launch_aux(which, ns, a, nblocks, s) : pcg_strict9::launch_aux(which, ns, a, nblocks, s);
+  const pcg::UnitEntry* u = find_unit(pcg::UNIT_STRICT, ns);
+  return u ? u->launch_aux(which, ns, a, nblocks, s) : cudaErrorInvalidValue;
 }
 }  // namespace pcg_strict
 namespace pcg_fast {
 cudaError_t upload_eos(int slot, const pcg::EosConst& e) {
-  cudaError_t r = slot == 0 ? pcg_fast1::upload_eos(slot, e) : pcg_fast9::upload_eos(slot, e);
-  if (r != cudaSuccess) return r;
-  return slot == 0 ? pcg_mixed1::upload_eos(slot, e) : pcg_mixed9::upload_eos(slot, e);
+  const int ns = slot == 0 ? 1 : e.nspec;
+  const pcg::UnitEntry* f = find_unit(pcg::UNIT_FAST, ns);
+  const pcg::UnitEntry* m = find_unit(pcg::UNIT_MIXED, ns);
+  if (!f || !m) return cudaErrorInvalidValue;
+  cudaError_t r = f->upload_eos(slot, e);
+  return r != cudaSuccess ? r : m->upload_eos(slot, e);
 }
 cudaError_t launch_stage(int stage, int ns, bool single, const pcg::StageArgs& a, int64_t nblocks, int variant,
                          cudaStream_t s) {
-  if (single)
-    return ns == 1 ? pcg_mixed1::launch_stage(stage, ns, single, a, nblocks, variant, s)
-                   : pcg_mixed9::launch_stage(stage, ns, single, a, nblocks, variant, s);
-  return ns == 1 ? pcg_fast1::launch_stage(stage, ns, single, a, nblocks, variant, s)
-                 : pcg_fast9::launch_stage(stage, ns, single, a, nblocks, variant, s);
+  const pcg::UnitEntry* u = find_unit(single ? pcg::UNIT_MIXED : pcg::UNIT_FAST, ns);
+  return u ? u->launch_stage(stage, ns, single, a, nblocks, variant, s) : cudaErrorInvalidValue;
 }
 cudaError_t launch_advance(int ns, const pcg::StageArgs& a, int64_t nblocks, int variant, cudaStream_t s) {
-  return ns == 1 ? pcg_fast1::launch_advance(ns, a, nblocks, variant, s)
-                 : pcg_fast9::launch_advance(ns, a, nblocks, variant, s);
+  const pcg::UnitEntry* u = find_unit(pcg::UNIT_FAST, ns);
+  return u ? u->launch_advance(ns, a, nblocks, variant, s) : cudaErrorInvalidValue;
 }
 }  // namespace pcg_fast
 
@@ -345,7 +367,8 @@ int check_array(const char* what, const pcg_array4* a, const IBox& b, int ncomp)
 
 int check_params(const pcg_hydro_params* p) {
   if (!p) return fail(PCG_EINVAL, "params is NULL");
-  if (p->nspec != 1 && p->nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d: kernels exist for 1 and 9", p->nspec);
+  if (!species_built(p->nspec))
+    return fail(PCG_EUNSUPPORTED, "nspec=%d: this build has kernels for %s species", p->nspec, species_list().c_str());
   if (p->ppm_type != 0 && p->ppm_type != 1) return fail(PCG_EINVAL, "PeleC::ppm_type must be 0 (PLM) or 1 (PPM)");
   if (p->use_hybrid_weno && p->ppm_type != 1)
     return fail(PCG_EINVAL, "PeleC::ppm_type must be 1 (PPM) to use WENO method");
@@ -554,7 +577,7 @@ void build_layout(Layout& L, const std::vector<BoxIn>& boxes, const pcg_hydro_pa
   L.esz = single ? 4 : 8;
   // the mixed form traces from TMA-staged shared-memory tiles of its FP32 primitive copy
   // (PPM without hybrid WENO, and PLM)
-  L.tile_trace = single && !prm->use_hybrid_weno;
+  L.tile_trace = single && !prm->use_hybrid_weno && pcg::trace_tile_species(ns);
   const int nt = pcg::nt_comps(ns), nf = pcg::nf_comps(ns), nv = pcg::nvar(ns), nq = pcg::qvar(ns);
   for (size_t r = 0; r < boxes.size(); ++r) {
     const BoxIn& B = boxes[r];
@@ -1014,6 +1037,14 @@ struct pcg_plan {
   int device = 0;
 };
 
+namespace pcg {
+// The message pcg_last_error returns, set by the other host units (pcg_fluxreg.cu).
+int set_error(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace pcg
+
 extern "C" {
 
 int pcg_init(int device) {
@@ -1042,7 +1073,9 @@ int pcg_set_eos_gamma(double gamma, double mw) {
 }
 
 int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid, const double* a_lo, const double* a_hi) {
-  if (nspec < 1 || nspec > pcg::MAXNS) return fail(PCG_EINVAL, "nspec must be in 1..%d", pcg::MAXNS);
+  if (nspec < 2 || nspec > pcg::MAXNS) return fail(PCG_EINVAL, "nspec must be in 2..%d", pcg::MAXNS);
+  if (!species_built(nspec))
+    return fail(PCG_EUNSUPPORTED, "nspec=%d: this build has kernels for %s species", nspec, species_list().c_str());
   if (!mw || !tmid || !a_lo || !a_hi) return fail(PCG_EINVAL, "NULL table");
   pcg::EosConst c{};
   c.kind = 1;
@@ -1075,6 +1108,15 @@ int pcg_set_eos_nasa7(int nspec, const double* mw, const double* tmid, const dou
     c.tmidf[k] = (float)c.tmid[k];
   }
   return store_eos(1, c);
+}
+
+int pcg_species_counts(int32_t* counts, int32_t max_counts) {
+  std::vector<int> v;
+  for (const pcg::UnitEntry& u : pcg::unit_table().units)
+    if (u.kind == pcg::UNIT_STRICT && species_built(u.ns)) v.push_back(u.ns);
+  std::sort(v.begin(), v.end());
+  for (int32_t k = 0; counts && k < max_counts && k < (int32_t)v.size(); ++k) counts[k] = v[k];
+  return (int)v.size();
 }
 
 int pcg_ctoprim(const pcg_hydro_params* prm, const int32_t lo[3], const int32_t hi[3], const pcg_array4* u,
@@ -1379,7 +1421,8 @@ int pcg_hydro_workspace(const pcg_hydro_params* prm, int32_t nbox, const int32_t
 }
 
 int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl, double* dt_out, pcg_stream_t stream) {
-  if (nspec != 1 && nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d", nspec);
+  if (!species_built(nspec))
+    return fail(PCG_EUNSUPPORTED, "nspec=%d: this build has kernels for %s species", nspec, species_list().c_str());
   if (nbox <= 0 || !boxes || !dt_out) return fail(PCG_EINVAL, "bad arguments");
   int rc = ensure_eos(nspec);
   if (rc) return rc;
@@ -1423,7 +1466,8 @@ int pcg_estdt(int32_t nspec, int32_t nbox, const pcg_box* boxes, double cfl, dou
 
 int pcg_update_state(int32_t nspec, int32_t nbox, const pcg_box* boxes, const pcg_array4* s_new, const double* dt,
                      pcg_stream_t stream) {
-  if (nspec != 1 && nspec != 9) return fail(PCG_EUNSUPPORTED, "nspec=%d", nspec);
+  if (!species_built(nspec))
+    return fail(PCG_EUNSUPPORTED, "nspec=%d: this build has kernels for %s species", nspec, species_list().c_str());
   if (nbox <= 0 || !boxes || !s_new) return fail(PCG_EINVAL, "bad arguments");
   int rc = ensure_eos(nspec);
   if (rc) return rc;
@@ -1747,7 +1791,7 @@ int pcg_reserve_workspace(int32_t device, int64_t bytes) {
 }
 
 int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage, int32_t variant) {
-  if (precision_mode < 0 || precision_mode > 2 || (nspec != 1 && nspec != 9) || stage < 0 || stage >= K_NSTAGE ||
+  if (precision_mode < 0 || precision_mode > 2 || !species_built(nspec) || stage < 0 || stage >= K_NSTAGE ||
       variant < 0 || variant > max_variant(precision_mode, stage))
     return fail(PCG_EINVAL, "launch variant (%d, %d, %d, %d) out of range", precision_mode, nspec, stage, variant);
   std::lock_guard<std::mutex> lk(g_var_mu);
@@ -1756,7 +1800,7 @@ int pcg_set_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage,
 }
 
 int pcg_get_launch_variant(int32_t precision_mode, int32_t nspec, int32_t stage) {
-  if (precision_mode < 0 || precision_mode > 2 || (nspec != 1 && nspec != 9) || stage < 0 || stage >= K_NSTAGE)
+  if (precision_mode < 0 || precision_mode > 2 || !species_built(nspec) || stage < 0 || stage >= K_NSTAGE)
     return fail(PCG_EINVAL, "launch variant query out of range");
   return variant_of(precision_mode, nspec, stage);
 }

@@ -53,6 +53,15 @@ SIGNATURES = {
     "pcg_last_error": ([], C.c_char_p),
     "pcg_set_eos_gamma": ([C.c_double, C.c_double], C.c_int),
     "pcg_set_eos_nasa7": ([C.c_int, _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(C.c_double)], C.c_int),
+    "pcg_species_counts": ([_P(C.c_int32), C.c_int32], C.c_int),
+    "pcg_fluxreg_create": ([C.c_int32, _I3, _I3, _I3, C.c_int32, C.c_int32, _I3, _I3, _P(_V)], C.c_int),
+    "pcg_fluxreg_info": ([_V, _P(C.c_int32), _P(C.c_int32)], C.c_int),
+    "pcg_fluxreg_reset": ([_V, _V], C.c_int),
+    "pcg_fluxreg_crse_add": ([_V, _I3, _I3, _A4, C.c_double, _V], C.c_int),
+    "pcg_fluxreg_fine_add": ([_V, _I3, _I3, _A4, C.c_double, _V], C.c_int),
+    "pcg_fluxreg_reflux": ([_V, _A4, C.c_double, _V], C.c_int),
+    "pcg_fluxreg_destroy": ([_V], C.c_int),
+    "pcg_average_down": ([_A4, _A4, _I3, _I3, C.c_int32, C.c_int32, _V], C.c_int),
     "pcg_ctoprim": ([_PRM, _I3, _I3, _A4, _A4, _A4, _V], C.c_int),
     "pcg_umdrv": ([_PRM, _I3, _I3, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _A4, _V], C.c_int),
     "pcg_srctoprim": ([_PRM, _I3, _I3, _A4, _A4, _A4, _A4, _V], C.c_int),

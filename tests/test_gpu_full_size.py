@@ -52,3 +52,33 @@ def test_one_step_of_a_closed_level_conserves(name, kw, prec):
         assert drift <= 1e-12 * ref, (name, c, drift, ref)
     assert float(st.dt.item()) > 0.0
     st.close()
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_fused_level_equals_per_box_at_full_size(prec):
+    """The 128^3 flame level advanced as one fused region (whose final-flux stage runs
+    its directions interleaved in z-slabs and whose prep, flux0 and flux2 launches run in
+    reverse order, the launch order of regions larger than L2) gives the hydro source of
+    the 64 boxes advanced as separate regions bit for bit in the plain FP64 form (box
+    independence: every output of a box depends on grow(box, 4) only, and the plain FP64
+    per-box form equals the oracle). In the mixed form, whose FP32 pressure offset p0 is
+    a per-region constant, within the mixed form's resolution."""
+    lev = wl.flame(n=128, box=32, seed=2)
+    out = []
+    for fuse in (False, True):
+        st = LevelStepper(lev, precision=prec, fuse=fuse, fused_tail=False)
+        st.fill()
+        st.plan.estdt(st.cfl, st.dt)
+        st.plan.hydro(st.dt)
+        torch.cuda.synchronize()
+        out.append(st.hsrc.data.clone())
+        st.close()
+        del st
+        torch.cuda.empty_cache()
+    if prec == abi.PREC_FP64:
+        assert torch.equal(out[0], out[1])
+    else:
+        from common import rel_errors
+
+        l1, _ = rel_errors(out[1].cpu().numpy(), out[0].cpu().numpy(), lev.nspec)
+        assert float(l1.max()) < 5e-4, l1  # the hydro-source bound of the mixed form

@@ -57,9 +57,9 @@ def set_variant(prec, nspec, stage, variant):
 def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES, state=None):
     """Time every variant of ``stages`` on ``plan`` (a hydro.Plan whose workspace holds
     a valid state; stages before each tuned one are run once first) and install the
-    fastest. With ``state`` (the device tensor the plan's boxes update) the fused step
-    tail is tuned too: whole ``plan.advance`` calls per variant, the state restored
-    afterwards. Returns {stage_name: {"variant": v, "ms": [ms per variant]}}."""
+    fastest. With ``state`` (the device tensor, or list of tensors, the plan's boxes
+    update) the fused step tail is tuned too: whole ``plan.advance`` calls per variant,
+    the state restored afterwards. Returns {stage_name: {"variant": v, "ms": [ms per variant]}}."""
     import torch
 
     prec, ns = plan.prm.precision_mode, plan.prm.nspec
@@ -67,10 +67,11 @@ def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES, state=None):
     torch.cuda.synchronize()
     result = {}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if state is not None:
+    states = [] if state is None else list(state) if isinstance(state, (list, tuple)) else [state]
+    if states:
         stages = tuple(stages) + (TAIL_STAGE,)
-        saved = state.clone()
-        dt_next = torch.zeros(1, dtype=torch.float64, device=state.device)
+        saved = [s.clone() for s in states]
+        dt_next = torch.zeros(1, dtype=torch.float64, device=states[0].device)
     for st in stages:
         times = []
         nv = n_variants(prec, st)
@@ -88,7 +89,8 @@ def tune(plan, dt_dev=None, reps=5, stages=TUNED_STAGES, state=None):
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / reps)
             if st == TAIL_STAGE:
-                state.copy_(saved)
+                for s, v0 in zip(states, saved):
+                    s.copy_(v0)
         best = min(range(nv), key=lambda v: times[v])
         set_variant(prec, ns, st, best)
         result[STAGE_NAMES[st]] = {"variant": best, "shape": describe(prec, st, best),

@@ -133,9 +133,9 @@ thread_local std::string g_err;
 constexpr int kTileVariant = 3;
 std::mutex g_var_mu;
 int g_variant[3][2][7] = {
-  {{0, 0, 2, 0, 2, 2, 2}, {2, 0, 1, 1, 2, 0, 2}},  // FP64 reference order
-  {{2, 0, 1, 0, 0, 0, 2}, {2, 0, 1, 0, 0, 0, 2}},  // FP64 with FMA
-  {{0, 0, 2, 0, 2, 0, 2}, {2, 0, 2, 2, 2, 1, 2}},  // mixed
+  {{0, 0, 2, 0, 1, 2, 1}, {2, 0, 1, 1, 1, 0, 2}},  // FP64 reference order
+  {{1, 0, 1, 0, 0, 0, 1}, {1, 0, 1, 0, 0, 0, 1}},  // FP64 with FMA
+  {{0, 0, 2, 0, 1, 0, 1}, {2, 0, 2, 2, 2, 1, 2}},  // mixed
 };
 int max_variant(int prec, int stage) { return (prec == PCG_PREC_MIXED && stage == K_TRACE) ? 5 : 2; }
 int variant_of(int prec, int ns, int stage) {

@@ -36,13 +36,13 @@ enum { K_LOWBC = K_NSTAGE, K_SRCQ, K_TRACE_TILE };
 // requests (__launch_bounds__ register caps); the host picks one per (form, species
 // count, stage) from a table the autotuner fills. 0 = no cap.
 constexpr int kMinBlocks[K_NSTAGE][3] = {
-  {0, 3, 5},  // ctoprim
+  {0, 5, 8},  // ctoprim
   {0, 0, 0},  // prep
   {0, 4, 5},  // trace
   {0, 6, 8},  // flux0
-  {4, 5, 6},  // flux1
+  {5, 6, 8},  // flux1
   {4, 5, 6},  // flux2
-  {0, 4, 5},  // consup: the caps apply to the fused step tail (k_advance)
+  {0, 5, 6},  // consup: the caps apply to the fused step tail (k_advance)
 };
 
 struct Item {

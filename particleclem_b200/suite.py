@@ -35,7 +35,7 @@ import sys
 
 import numpy as np
 
-from . import abi, roofline as rl, workloads as wl
+from . import abi, autotune, roofline as rl, workloads as wl
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -98,11 +98,16 @@ def batch_workload(nbox=512, steps=10, warmup=3, device=0):
     res = {}
     states = {}
     launches = None
+    tuned = {}
     for name, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
         bb = BoxBatch(patches, eos, precision=prec, device=device)
         bb.step()  # one step from the initial state, kept for the error
         torch.cuda.synchronize()
         states[name] = [s.data.clone() for s in bb.states]
+        # launch shapes tuned for this batch's box sizes (both forms), the previous
+        # table restored afterwards
+        keep = {st: autotune.get_variant(prec, 9, st) for st in autotune.TUNED_STAGES + (autotune.TAIL_STAGE,)}
+        tuned[name] = autotune.tune(bb.plan, bb.dt, reps=3, state=[s.data for s in bb.states])
         bb.capture()
         launches = bb.launches_per_step
         ms = _timed(torch, bb.replay, steps, warmup)
@@ -110,6 +115,8 @@ def batch_workload(nbox=512, steps=10, warmup=3, device=0):
                      "path_hbm_frac": balg / (ms / 1e3) / 1e9 / pk["hbm_gbs"]}
         bb.close()
         del bb
+        for st, v in keep.items():
+            autotune.set_variant(prec, 9, st, v)
         torch.cuda.empty_cache()
     g = abi.NGROW
     a = torch.cat([x[:, g:-g, g:-g, g:-g].reshape(x.shape[0], -1) for x in states["fp64"]], dim=1)
@@ -120,7 +127,8 @@ def batch_workload(nbox=512, steps=10, warmup=3, device=0):
             "speedup_mixed_over_fp64": res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"],
             "error_mixed_vs_fp64_one_step": {"s_new_max_rel_l1": float(l1.max()), "s_new_max_rel_linf": float(li.max()),
                                              "normalisation": "per physical group"},
-            "launches_per_step": launches, "b_alg_bytes_per_step": balg, "peak_source": pk["source"]}
+            "launches_per_step": launches, "b_alg_bytes_per_step": balg, "peak_source": pk["source"],
+            "launch_tuning": tuned}
 
 
 def run_batch(args):

@@ -21,7 +21,10 @@ CASES = {
     "one_box": (12, 2, [((6, 4, 8), (17, 19, 15))]),
     "wrap_and_abutting": (12, 2, [((0, 8, 4), (7, 15, 11)), ((8, 8, 4), (15, 15, 11))]),
     "ratio4": (12, 4, [((16, 12, 20), (27, 23, 31))]),
+    # the coarse level in four boxes (CrseAdd per coarse box), the fine box across them
+    "coarse_boxes": (12, 2, [((8, 8, 4), (15, 15, 11))]),
 }
+COARSE_SPLIT = {"coarse_boxes": 2}  # boxes per direction in x and y
 CONSERVED = (abi.URHO, abi.UMX, abi.UMY, abi.UMZ, abi.UEDEN)
 
 
@@ -94,13 +97,18 @@ def two_level(case, seed=11, backend=None, do_reflux=True, record=None):
     o.set_eos(eos)
     dt_c = 0.3 * o.estdt(dom[0], dom[1], lev.box_fab(*dom), dx_c)
     reg = be.Register(abi.nvar(1), dom[0], dom[1], (1, 1, 1), ratio, fine)
-    # coarse step
+    # coarse step, box by box
     prm_c = abi.make_params(dx_c, dt_c, 1, dom[0], dom[1], (0, 0, 0), (0, 0, 0))
-    hs, flx = be.hydro(prm_c, dom[0], dom[1], lev.box_fab(*dom))
-    reg.crse_add(dom[0], dom[1], flx, dt_c)
-    if record is not None:
-        record.append(("crse", dom[0], dom[1], flx, dt_c))
-    new_c = be.update(dom[0], dom[1], lev.box_fab(*dom), hs, dt_c)
+    m = COARSE_SPLIT.get(case, 1)
+    e = n // m
+    cboxes = [((a * e, b * e, 0), (a * e + e - 1, b * e + e - 1, n - 1)) for b in range(m) for a in range(m)]
+    new_c = np.empty_like(lev.fab.view(*dom))
+    for lo, hi in cboxes:
+        hs, flx = be.hydro(prm_c, lo, hi, lev.box_fab(lo, hi))
+        reg.crse_add(lo, hi, flx, dt_c)
+        if record is not None:
+            record.append(("crse", lo, hi, flx, dt_c))
+        new_c[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = be.update(lo, hi, lev.box_fab(lo, hi), hs, dt_c)
     # fine substeps: ghost cells from the fine boxes where they exist, else injected from
     # the old coarse state
     dt_f = dt_c / ratio

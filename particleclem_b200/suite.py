@@ -149,6 +149,14 @@ def sweep_workload(n=256, box=64, steps=100, every=10, schemes=(1, 0), device=0)
     for ppm in schemes:
         a = LevelStepper(lev0, precision=abi.PREC_FP64, fuse=False, ppm_type=ppm, device=device)
         b = LevelStepper(lev0, precision=abi.PREC_MIXED, fuse=True, ppm_type=ppm, device=device)
+        # launch shapes tuned on each form's own plan for this level (one species), the
+        # previous table restored after the measurement
+        keep, tuned = {}, {}
+        for name, st in (("fp64", a), ("mixed", b)):
+            prec = st.prm.precision_mode
+            keep[prec] = {k: autotune.get_variant(prec, 1, k) for k in autotune.TUNED_STAGES + (autotune.TAIL_STAGE,)}
+            st.step()
+            tuned[name] = autotune.tune(st.plan, st.dt, reps=3, state=st.state.data)
         a.capture()
         b.capture()
         ms_a = _timed(torch, a.replay, 3, 2)
@@ -174,8 +182,11 @@ def sweep_workload(n=256, box=64, steps=100, every=10, schemes=(1, 0), device=0)
                     "fp64_ms_per_step": ms_a, "mixed_ms_per_step": ms_b,
                     "fp64_cell_updates_per_s": lev0.ncells() / (ms_a / 1e3),
                     "mixed_cell_updates_per_s": lev0.ncells() / (ms_b / 1e3),
-                    "speedup_mixed_over_fp64": ms_a / ms_b,
+                    "speedup_mixed_over_fp64": ms_a / ms_b, "launch_tuning": tuned,
                     "error_components": "rho, rho u, rho v, rho w, rho E (per physical group)", "growth": growth})
+        for prec, table in keep.items():
+            for k, v in table.items():
+                autotune.set_variant(prec, 1, k, v)
         a.close()
         b.close()
         del a, b

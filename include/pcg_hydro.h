@@ -329,8 +329,8 @@ int pcg_fluxreg_fine_add(pcg_fluxreg* reg, const int32_t lo[3], const int32_t hi
  * PeleC's post_timestep does. */
 int pcg_fluxreg_reflux(pcg_fluxreg* reg, pcg_array4* s_crse, double vol, pcg_stream_t stream);
 int pcg_fluxreg_destroy(pcg_fluxreg* reg);
-/* avgDown on regular boxes (PeleC::avgDown, Source/PeleC.cpp after :1091; AMReX's
- * average_down): every coarse cell under the fine box [fine_lo, fine_hi] becomes the mean
+/* avgDown on regular boxes (PeleC::avgDown, Source/PeleC.cpp:1440, called at :1098;
+ * AMReX's average_down): every coarse cell under the fine box [fine_lo, fine_hi] becomes the mean
  * of its ratio^3 fine cells, components 0..ncomp-1. */
 int pcg_average_down(const pcg_array4* fine, pcg_array4* crse, const int32_t fine_lo[3], const int32_t fine_hi[3],
                      int32_t ratio, int32_t ncomp, pcg_stream_t stream);

@@ -6,7 +6,7 @@ Source/PeleC.cpp:1343-1400: CrseAdd on the coarse level, FineAdd on every fine s
 resets the register at the start of the coarse step (Source/Advance.cpp:30-31) and, after
 the fine subcycles, corrects the coarse cells next to the fine region
 (PeleC::reflux, Source/PeleC.cpp:1403-1414) before averaging the fine level down onto the
-coarse cells it covers (PeleC::avgDown). ``FluxRegister`` and ``average_down`` are those
+coarse cells it covers (PeleC::avgDown, Source/PeleC.cpp:1440, called at :1098). ``FluxRegister`` and ``average_down`` are those
 steps on the device (include/pcg_hydro.h, pcg_fluxreg_* and pcg_average_down).
 """
 from __future__ import annotations

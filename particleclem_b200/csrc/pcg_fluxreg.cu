@@ -5,7 +5,8 @@
 // after the hydro source (Source/Hydro.cpp:281-287) with the area-weighted fluxes and the
 // cell volume as "dx"; the register is reset at the start of the coarse advance
 // (Source/Advance.cpp:30-31) and applied in PeleC::reflux (Source/PeleC.cpp:1403-1414)
-// after the fine subcycles, before avgDown (:1091-...). The register class itself is
+// after the fine subcycles, from post_timestep (:1090-1092), before avgDown (:1098,
+// defined at :1440). The register class itself is
 // AMReX's EBFluxRegister / YAFluxRegister (not in the reference checkout); on regular
 // boxes it implements the conservative refluxing of Berger & Colella (J. Comput. Phys.
 // 82, 1989), restated here:

@@ -5,6 +5,8 @@
 //   pc_ctoprim's launch      (Source/Hydro.cpp:104-116) by pcg_ctoprim,
 //   pc_srctoprim's launch    (Source/Hydro.cpp:161-174) by pcg_srctoprim,
 //   pc_umdrv                 (Source/Hydro.cpp:245-249) by pcg_umdrv,
+//   update_flux_registers    (Source/Hydro.cpp:281-287) and reflux
+//                            (Source/PeleC.cpp:1403-1414) by the library's register,
 // passing its FABs as pcg_array4 descriptors: same addressing as amrex::Array4, no
 // copies. It needs only amrex::Array4, amrex::GpuArray and amrex::Real from AMReX (the
 // repository's tests compile it against a small AMReX-API shim).
@@ -81,6 +83,29 @@ inline int umdrv(amrex::Box const& bx, const int* domlo, const int* domhi, const
     ar[d] = to_array4(a[d]);
   }
   return pcg_umdrv(&prm, lo, hi, &u, &uo, &qq, &qa, &sq, fl, ar, &vv, stream);
+}
+
+// PeleC::update_flux_registers (Source/PeleC.cpp:1343-1400) for regular boxes, on the
+// library's register: fr_as_crse is the register of the level above (nullptr on the
+// finest level), fr_as_fine the register of this level (nullptr on level 0). flux: the
+// box's three area-weighted flux FABs. (The reference passes the cell volume as "dx";
+// the library's calls take the area-weighted fluxes directly.)
+inline int update_flux_registers(pcg_fluxreg* fr_as_crse, pcg_fluxreg* fr_as_fine, amrex::Box const& bx,
+                                 amrex::Array4<const amrex::Real> const* flux, amrex::Real dt, pcg_stream_t stream) {
+  const int32_t lo[3] = {bx.smallEnd(0), bx.smallEnd(1), bx.smallEnd(2)};
+  const int32_t hi[3] = {bx.bigEnd(0), bx.bigEnd(1), bx.bigEnd(2)};
+  const pcg_array4 f[3] = {to_array4(flux[0]), to_array4(flux[1]), to_array4(flux[2])};
+  int rc = PCG_OK;
+  if (fr_as_crse) rc = pcg_fluxreg_crse_add(fr_as_crse, lo, hi, f, dt, stream);
+  if (rc == PCG_OK && fr_as_fine) rc = pcg_fluxreg_fine_add(fr_as_fine, lo, hi, f, dt, stream);
+  return rc;
+}
+
+// PeleC::reflux (Source/PeleC.cpp:1403-1414) on one coarse FAB that holds every cell the
+// register corrects; vol: the coarse cell volume.
+inline int reflux(pcg_fluxreg* reg, amrex::Array4<amrex::Real> const& s_crse, amrex::Real vol, pcg_stream_t stream) {
+  pcg_array4 s = to_array4(s_crse);
+  return pcg_fluxreg_reflux(reg, &s, vol, stream);
 }
 
 }  // namespace pcg_pelec

@@ -122,3 +122,25 @@ def test_species_counts_of_the_build():
     assert _rc("pcg_set_eos_nasa7", 1, *ptrs) == -1
     prm = abi.make_params((1, 1, 1), 0.1, missing, (0, 0, 0), (7, 7, 7), (0, 0, 0), (0, 0, 0))
     assert _rc("pcg_hydro_box", C.byref(prm), abi.ivec((0, 0, 0)), abi.ivec((7, 7, 7)), None, None, None, None) == -4
+
+
+def test_species_build_options(monkeypatch):
+    """PCG_NSPEC parsing of the build: sorted unique counts, the EOS bank sized to the
+    largest (even, at least 16), one strict/fast/mixed unit per count plus the host units;
+    bad lists are refused."""
+    from particleclem_b200 import build
+
+    monkeypatch.setenv("PCG_NSPEC", "9, 1,53,9")
+    assert build.species_counts() == (1, 9, 53)
+    assert build.max_species((1, 9, 53)) == 54
+    assert build.max_species((1, 2, 9)) == 16
+    tags = [u[0] for u in build.units((1, 9, 53))]
+    assert tags[:3] == ["strict_ns53", "fast_ns53", "mixed_ns53"]  # largest units start first
+    assert sorted(tags) == sorted([f"{k}_ns{n}" for n in (1, 9, 53) for k in ("strict", "fast", "mixed")]
+                                  + ["host", "fluxreg"])
+    assert all("-DPCG_MAXNS=54" in u[2] for u in build.units((1, 9, 53)) if u[0] != "fluxreg")
+    monkeypatch.setenv("PCG_NSPEC", "0,9")
+    with pytest.raises(ValueError):
+        build.species_counts()
+    monkeypatch.delenv("PCG_NSPEC")
+    assert build.species_counts() == build.DEFAULT_NSPEC

@@ -304,7 +304,8 @@ int pcg_reserve_workspace(int32_t device, int64_t bytes);
  * direction, boxes aligned to the ratio, inside the coarse domain, disjoint). It holds
  * one accumulator of ncomp doubles per coarse face on the coarse/fine boundary (faces on
  * non-periodic domain boundaries and between fine boxes have none). All calls are on the
- * device current at creation; the register owns its device memory. */
+ * device current at creation (a call with another device current returns PCG_EINVAL);
+ * the register owns its device memory. */
 typedef struct pcg_fluxreg pcg_fluxreg;
 int pcg_fluxreg_create(int32_t ncomp, const int32_t crse_domlo[3], const int32_t crse_domhi[3],
                        const int32_t periodic[3], int32_t ratio, int32_t nfine, const int32_t* fine_lo /*[3*nfine]*/,

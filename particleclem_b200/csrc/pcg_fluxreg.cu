@@ -174,6 +174,22 @@ bool covers_faces(const pcg_array4* f, const int lo[3], const int hi[3], int nc)
 constexpr int kThreads = 128;
 int blocks(int64_t n) { return int((n + kThreads - 1) / kThreads); }
 
+// The register's device memory belongs to the device that was current at creation: a
+// call made with another device current would hand that device foreign pointers.
+int check_device(const pcg_fluxreg* R);
+
+}  // namespace
+
+namespace {
+int check_device(const pcg_fluxreg* R) {
+  int cur = -1;
+  const cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return cuda_err(e, "fluxreg: cudaGetDevice");
+  if (cur != R->device)
+    return err(PCG_EINVAL, "fluxreg: the register was created on device %lld, the current device is %lld",
+               R->device, cur);
+  return PCG_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -313,6 +329,7 @@ int pcg_fluxreg_info(const pcg_fluxreg* R, int32_t* nfaces, int32_t* ncells) {
 
 int pcg_fluxreg_reset(pcg_fluxreg* R, pcg_stream_t stream) {
   if (!R) return err(PCG_EINVAL, "fluxreg: NULL register");
+  if (int rc = check_device(R)) return rc;
   if (R->ne == 0) return PCG_OK;
   const cudaError_t e = cudaMemsetAsync(R->d_acc, 0, size_t(R->ne) * R->ncomp * sizeof(double),
                                         reinterpret_cast<cudaStream_t>(stream));
@@ -322,6 +339,7 @@ int pcg_fluxreg_reset(pcg_fluxreg* R, pcg_stream_t stream) {
 int pcg_fluxreg_crse_add(pcg_fluxreg* R, const int32_t lo[3], const int32_t hi[3], const pcg_array4* flx,
                          double dt, pcg_stream_t stream) {
   if (!R || !lo || !hi || !flx) return err(PCG_EINVAL, "fluxreg: NULL argument");
+  if (int rc = check_device(R)) return rc;
   const int l[3] = {lo[0], lo[1], lo[2]}, h[3] = {hi[0], hi[1], hi[2]};
   if (h[0] < l[0] || h[1] < l[1] || h[2] < l[2]) return err(PCG_EINVAL, "fluxreg: empty coarse box");
   if (!covers_faces(flx, l, h, R->ncomp))
@@ -337,6 +355,7 @@ int pcg_fluxreg_crse_add(pcg_fluxreg* R, const int32_t lo[3], const int32_t hi[3
 int pcg_fluxreg_fine_add(pcg_fluxreg* R, const int32_t lo[3], const int32_t hi[3], const pcg_array4* flx,
                          double dt, pcg_stream_t stream) {
   if (!R || !lo || !hi || !flx) return err(PCG_EINVAL, "fluxreg: NULL argument");
+  if (int rc = check_device(R)) return rc;
   int box = -1;
   for (int b = 0; b < R->nfine && box < 0; ++b)
     if (std::equal(lo, lo + 3, R->flo.begin() + 3 * b) && std::equal(hi, hi + 3, R->fhi.begin() + 3 * b)) box = b;
@@ -354,6 +373,7 @@ int pcg_fluxreg_fine_add(pcg_fluxreg* R, const int32_t lo[3], const int32_t hi[3
 int pcg_fluxreg_reflux(pcg_fluxreg* R, pcg_array4* s_crse, double vol, pcg_stream_t stream) {
   if (!R || !s_crse) return err(PCG_EINVAL, "fluxreg: NULL argument");
   if (!(vol > 0.0)) return err(PCG_EINVAL, "fluxreg: the coarse cell volume must be > 0");
+  if (int rc = check_device(R)) return rc;
   if (R->ne == 0) return PCG_OK;
   if (!covers_box(s_crse, R->clo, R->chi, R->ncomp))
     return err(PCG_EINVAL, "fluxreg: the coarse state must cover the register's cells with %lld components",

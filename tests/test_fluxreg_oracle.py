@@ -190,3 +190,24 @@ def test_fluxreg_argument_errors():
     assert _create(8, *dom, (1, 1, 1), 2, [((20, 0, 0), (27, 7, 7))]) == -1  # outside the coarse domain
     assert _create(8, *dom, (1, 1, 1), 1, [((0, 0, 0), (7, 7, 7))]) == -1
     assert _create(0, *dom, (1, 1, 1), 2, [((0, 0, 0), (7, 7, 7))]) == -1
+
+
+def test_average_down_argument_errors():
+    """pcg_average_down refuses a fine box off the ratio grid, a bad ratio or component
+    count, and arrays that do not cover the boxes, before any device work."""
+    lib = native.load()
+    fine = abi.Fab(np.zeros((8, 8, 8, 8)), (0, 0, 0))
+    crse = abi.Fab(np.zeros((8, 4, 4, 4)), (0, 0, 0))
+
+    def rc(flo, fhi, ratio=2, nc=8, f=fine, c=crse):
+        return lib.pcg_average_down(C.byref(abi.array4(f)), C.byref(abi.array4(c)), abi.ivec(flo), abi.ivec(fhi),
+                                    ratio, nc, None)
+
+    assert rc((1, 0, 0), (6, 7, 7)) == -1
+    assert "aligned" in lib.pcg_last_error().decode()
+    assert rc((0, 0, 0), (7, 7, 7), ratio=1) == -1
+    assert rc((0, 0, 0), (7, 7, 7), nc=0) == -1
+    assert rc((0, 0, 0), (7, 7, 7), nc=9) == -1  # more components than the arrays hold
+    assert rc((0, 0, 0), (15, 7, 7)) == -1  # the fine array does not cover the box
+    small = abi.Fab(np.zeros((8, 2, 2, 2)), (0, 0, 0))
+    assert rc((0, 0, 0), (7, 7, 7), c=small) == -1  # the coarse array does not cover it
